@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the plain FP64 Lax-Friedrichs hot path on B200.
+
+Workload (one "step" = one time step of Solver::Advance + the adaptive dt
+update): the coaxial channel r1 = 0.2, r2 = 0.8 on the 1600 x 640 grid, IC
+rho = 1, v_z = 0.1, p = beta/2, B_phi = r1/r, inlet fixed, zero-gradient
+outlet, slip walls, CFL 0.4, FP64 (fast precision: reciprocal multiplies +
+FMA, <= 1e-12 of the reference after 1000 steps).  Inputs are synthetic and
+built on the host from the configuration.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: a single grid does not shard (one domain per GPU); N ranks run
+N independent replicas and ``value`` adds their cell updates ("replicas only").
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L_MAX, M_MAX = 1600, 640
+CELLS = L_MAX * (M_MAX + 1)          # interior cell updates per step
+ALG_BYTES_PER_CELL = 128             # 8 FP64 conserved values read + 8 written
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--cpu-child", type=str, default="", help=argparse.SUPPRESS)
+    ap.add_argument("--profile", action="store_true",
+                    help="lean run for ncu: warm-up, then --steps eager time steps, no extras")
+    ap.add_argument("--precision", choices=("fast", "exact"), default="fast")
+    return ap.parse_args()
+
+
+def workload_config():
+    return {"workload": "plain FP64 LF time step, coaxial channel 1600x640 (config 2 grid)",
+            "L_max": L_MAX, "M_max": M_MAX, "cells_per_step": CELLS, "cfl": 0.4,
+            "adaptive_dt": True, "precision": "fast", "geometry": "r1=0.2, r2=0.8",
+            "l2": "per-step working set 138 MB (8 planes read + 8 written) > 126 MB L2, no flush",
+            "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------- CPU side
+def _case():
+    from tests import cases
+    return cases.channel_case(L=L_MAX, M=M_MAX)
+
+
+def cpu_child(spec: str) -> None:
+    """Runs in a subprocess so OMP_NUM_THREADS applies: time the reference
+    CPU build (or the oracle port) on the workload and print JSON."""
+    kind, steps, warmup = spec.split(":")
+    steps, warmup = int(steps), int(warmup)
+    from oracle import bind
+    case = _case()
+    be = bind.Ref(case.oracle_dict()) if kind == "reference" else bind.Port(case.oracle_dict())
+    cfg = case.cfg
+    dt = cfg.dt
+    for _ in range(warmup):
+        be.advance(dt)
+        dt = be.compute_dt(cfg.cfl_number, cfg.dt_growth_factor, cfg.dt_min, cfg.dt_max, dt)
+    t0 = time.perf_counter()
+    per = []
+    for _ in range(steps):
+        s0 = time.perf_counter()
+        be.advance(dt)
+        dt = be.compute_dt(cfg.cfl_number, cfg.dt_growth_factor, cfg.dt_min, cfg.dt_max, dt)
+        per.append(time.perf_counter() - s0)
+    el = time.perf_counter() - t0
+    print(json.dumps({"seconds": el, "steps": steps, "per_step": per}))
+
+
+def run_cpu(kind: str, steps: int, warmup: int, threads: int) -> dict:
+    env = dict(os.environ)
+    env.update(OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores")
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--cpu-child",
+                          f"{kind}:{steps}:{warmup}"], capture_output=True, text=True, env=env,
+                         timeout=1800)
+    if out.returncode != 0:
+        raise RuntimeError(out.stderr[-2000:])
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def cpu_kind():
+    from oracle import bind
+    return "reference" if bind.ref_available() else "port"
+
+
+def cpu_baseline_leg() -> dict:
+    kind = cpu_kind()
+    threads = os.cpu_count() or 1
+    probe = run_cpu(kind, 2, 1, threads)
+    per = probe["seconds"] / probe["steps"]
+    steps = max(3, min(200, int(20.0 / max(per, 1e-6))))   # ~20 s of CPU work
+    res = run_cpu(kind, steps, 1, threads)
+    value = CELLS * res["steps"] / res["seconds"]
+    return {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+            "sample": f"{res['steps']} time steps of the 1600x640 channel "
+                      f"(OMP_NUM_THREADS={threads}, OMP_PROC_BIND=close)"}
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_uuid: str | None):
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.uuid = device_uuid
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+               "-lms", "100"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(cmd, stdout=self.fh, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per interior-kernel launch from the committed ncu summary."""
+    p = ROOT / "profiles" / "lf_fast_kernel_1600x640.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------- GPU side
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local_rank))
+
+    case = _case()
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+    stream = torch.cuda.ExternalStream(solver.stream_handle())
+
+    # warm-up (includes the exact first step and the graph build)
+    solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=max(args.warmup, 1))
+    _, step0 = solver.time()
+    dt_now = solver.ComputeDt(cfg.dt)
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res = solver.run(T=1e300, dt=dt_now, adaptive=True, max_steps=args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    t_max = ms
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    assert res.steps == args.steps, res
+
+    # roofline of the dominant kernel: live CUDA events per launch
+    int_ms, bc_ms = solver.profile_kernels(50, res.dt)
+    hbm, hbm_src = measured_hbm()
+    achieved = ALG_BYTES_PER_CELL * CELLS / (int_ms * 1e-3) / 1e9
+    traffic = profiled_traffic()
+
+    # end to end through the C ABI with host buffers: the reference driver's
+    # per-step pattern (Advance, then ComputeDt back on the host), with the
+    # initial state uploaded from and the final state read into pinned memory
+    import numpy as np
+    lib = solver.lib
+    shape = (10,) + solver.shape
+    h_in = torch.from_numpy(np.ascontiguousarray(case.phys)).pin_memory()
+    h_out = torch.empty((8,) + solver.shape, dtype=torch.float64).pin_memory()
+    n_e2e = args.steps
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    solver.set_physical(h_in.numpy())
+    dt = cfg.dt
+    for _ in range(n_e2e):
+        solver.Advance(dt)
+        dt = solver.ComputeDt(dt)
+    for k in range(8):
+        lib.mpd_download(solver.h, k, ctypes.cast(ctypes.c_void_p(h_out[k].data_ptr()),
+                                                  pkg._native.DP))
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    plane = solver.shape[0] * solver.shape[1] * 8
+    h2d = (10 * plane + 8 * n_e2e) / n_e2e          # IC planes + dt per step
+    d2h = (8 * plane) / n_e2e + 8                   # final state + dt per step
+    solver.close()
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1:
+            try:
+                cpu = cpu_baseline_leg()
+            except Exception as exc:  # noqa: BLE001 - report, do not fail the bench
+                cpu = {"value": None, "unit": "cell-updates/s", "cores": os.cpu_count(),
+                       "kind": cpu_kind(), "sample": f"failed: {exc}"[:300]}
+        value = world * CELLS * args.steps / (t_max * 1e-3)
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "kernel": "lf_fast_kernel", "kernel_ms": int_ms,
+                         "bc_kernel_ms": bc_ms, "peak_source": hbm_src},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * CELLS * n_e2e / e2e_s, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+        }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def run_profile(args):
+    """Lean run for profilers: the exact first step, --warmup graph steps, then
+    --steps eagerly launched steps (interior + boundary kernel each)."""
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    case = _case()
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision=args.precision)
+    solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=max(args.warmup, 1))
+    dt = solver.ComputeDt(cfg.dt)
+    for _ in range(args.steps):
+        solver.Advance(dt)
+    t, step = solver.time()
+    solver.close()
+    print(json.dumps({"profile_steps": args.steps, "step": step, "t": t}))
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    kind = cpu_kind()
+    probe = run_cpu(kind, 1, 0, threads)
+    per = max(probe["seconds"], 1e-6)
+    steps = max(1, min(args.steps, int(150.0 / per)))   # bounded: a few minutes at most
+    warm = min(args.warmup, 3)
+    res = run_cpu(kind, steps, warm, threads)
+    value = CELLS * res["steps"] / res["seconds"]
+    return {
+        "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+        "n_gpus": world, "steps": res["steps"], "warmup": warm,
+        "ms_per_step": 1e3 * res["seconds"] / res["steps"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(),
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+                         "sample": f"{res['steps']} of the requested {args.steps} time steps"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    if args.cpu_child:
+        cpu_child(args.cpu_child)
+        return
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.profile:
+        run_profile(args)
+        return
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        line = run_ours(args, rank, world, local_rank)
+    if line is not None:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

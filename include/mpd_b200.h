@@ -1,0 +1,215 @@
+/*
+ * mpd_b200 — C ABI of the B200 Lax-Friedrichs MHD solver.
+ *
+ * One opaque handle owns one solve: device-resident structure-of-arrays FP64
+ * storage of the eight conserved planes (ping-pong), the initial physical
+ * planes, the wall profiles, the compiled boundary-condition table and one
+ * CUDA stream.  Every entry point returns an int status (MPD_OK = 0) and never
+ * throws; mpd_last_error() gives the message of the calling thread's last
+ * failure.  One host thread drives a handle at a time.
+ *
+ * Index conventions follow the reference exactly (single MPI rank):
+ *   planes are (L_max+2) x (M_max+3) doubles, row-major [l][m];
+ *   l = 0 and l = L_max+1 are ghost rows, m = 0 and m = M_max+2 ghost columns;
+ *   interior l in [1, L_max] (z = (l-1)*dz), m in [1, M_max+1] (m_global = m-1).
+ * Host planes passed in or out of this ABI are dense with that shape.
+ *
+ * The reference exposes C++ classes, not a C API; each entry point below names
+ * the reference member it replaces (paths relative to the reference repo).
+ */
+#ifndef MPD_B200_H
+#define MPD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MPD_OK 0
+#define MPD_ERR_INVALID 1        /* bad argument or configuration              */
+#define MPD_ERR_CUDA 2           /* a CUDA runtime call failed                  */
+#define MPD_ERR_NOMEM 3          /* device or pinned allocation failed / budget */
+#define MPD_ERR_UNSUPPORTED_BC 4 /* boundary configuration the device can't run */
+#define MPD_ERR_EXPR 5           /* expression failed to compile                */
+#define MPD_ERR_NONFINITE 6      /* NaN or Inf seen in the state                */
+#define MPD_ERR_TIMEOUT 7        /* a bounded device wait gave up               */
+#define MPD_ERR_NO_DEVICE 8      /* no CUDA device / extension unusable         */
+
+/* ---- enumerations (values equal the reference's enums) ----------------- */
+/* FaceBC::Face, include/face_bc.hpp:52 */
+enum { MPD_FACE_L_LO = 0, MPD_FACE_L_HI = 1, MPD_FACE_M_LO = 2, MPD_FACE_M_HI = 3 };
+/* FieldCondType, include/field_condition.hpp:92-97 */
+enum { MPD_NEUMANN = 0, MPD_DIRICHLET = 1, MPD_EXPRESSION = 2, MPD_AXIS_LF = 3 };
+/* Fields physical members, include/fields.hpp:35-37 */
+enum {
+    MPD_RHO = 0, MPD_V_Z = 1, MPD_V_R = 2, MPD_V_PHI = 3, MPD_E = 4,
+    MPD_P_GAS = 5, MPD_P_TOT = 6, MPD_H_Z = 7, MPD_H_R = 8, MPD_H_PHI = 9
+};
+/* arithmetic of the plain FP64 path */
+enum {
+    MPD_PRECISION_EXACT = 0, /* same IEEE operations, order and true divides as the
+                                reference: bit-for-bit identical fields        */
+    MPD_PRECISION_FAST = 1   /* reciprocal multiplies + FMA in the interior update
+                                (<= 1e-12 relative L-inf after 1000 steps)     */
+};
+
+/* ---- configuration ----------------------------------------------------- */
+/* FieldCond, include/field_condition.hpp:100-105 */
+typedef struct mpd_field_cond {
+    int type;          /* MPD_NEUMANN / MPD_DIRICHLET / MPD_EXPRESSION / MPD_AXIS_LF */
+    double value;      /* Neumann offset or Dirichlet value                          */
+    const char *expr;  /* expression source (MPD_EXPRESSION only), NUL-terminated    */
+} mpd_field_cond;
+
+/* BCSegmentConfig, include/config.hpp:82-95 (same field order) */
+typedef struct mpd_bc_segment {
+    int global_lo;     /* negative -> face start */
+    int global_hi;     /* negative -> face end   */
+    mpd_field_cond rho, v_z, v_r, v_phi, e, H_z, H_r, H_phi;
+} mpd_bc_segment;
+
+/* The SimConfig fields the hot path reads (include/config.hpp:119-176) plus
+ * Grid::r_0 (include/grid.hpp:38).  dz and dy are passed as computed by the
+ * caller (SimConfig::Init, src/config.cpp:15-18: 1/L_max, 1/M_max). */
+typedef struct mpd_config {
+    double gamma, beta, H_z0;
+    int L_max, M_max;
+    double dz, dy;
+    double r_0;
+    int n_segments[4];                    /* per face, indexed by MPD_FACE_*  */
+    const mpd_bc_segment *segments[4];    /* in config order                  */
+    int precision;                        /* MPD_PRECISION_*                  */
+    int with_prev;                        /* keep prev planes for SolutionChange */
+} mpd_config;
+
+/* IGeometry sampled on the host at z = (l-1)*dz for l = 0..L_max+1
+ * (include/igeometry.hpp:16-34, used by Grid::Build src/grid.cpp:20-42). */
+typedef struct mpd_geometry {
+    const double *r_inner, *r_outer, *dr_inner_dz, *dr_outer_dz;
+} mpd_geometry;
+
+typedef struct mpd_solver mpd_solver;
+
+/* ---- lifetime ---------------------------------------------------------- */
+/* Replaces the Fields ctor + Fields::InitConservative (src/fields.cpp:40-57),
+ * Grid::Build and the Solver ctor (src/solver.cpp:9-16: FaceBC::FromConfig,
+ * PerFieldBC validation and expression compile).  phys10 is the initial
+ * physical state written by IInitialCondition::Apply: 10 dense host planes in
+ * MPD_RHO..MPD_H_PHI order (ghost entries are ignored and treated as 0). */
+int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *phys10,
+               mpd_solver **out);
+void mpd_destroy(mpd_solver *s);
+const char *mpd_last_error(void);
+
+/* ---- the hot path -------------------------------------------------------- */
+/* Solver::Advance(double dt), src/solver.cpp:22-37.  Enqueued on the handle's
+ * stream; returns without waiting.  Also records the maximum wave speed of the
+ * new state (for mpd_compute_dt) and the L-inf residual of the step. */
+int mpd_advance(mpd_solver *s, double dt);
+
+/* Graph-resident driver loop of src/main.cpp:191-282: T clamp, adaptive dt
+ * (Diagnostics::ComputeDt after every step), the reference's relative-L2
+ * convergence check every check_frequency steps, and an L-inf residual
+ * criterion.  Runs until t >= T, convergence, or max_steps. */
+typedef struct mpd_run_params {
+    double T;                   /* end time (use a huge value for step-limited runs) */
+    double dt;                  /* initial dt (SimConfig::dt)                         */
+    int adaptive;               /* SimConfig::adaptive_dt                             */
+    double cfl_number, dt_growth_factor, dt_min, dt_max;
+    double convergence_threshold; /* relative-L2 change threshold, 0 = off          */
+    int check_frequency;          /* steps between SolutionChange checks             */
+    double residual_tol;          /* stop when the L-inf residual <= tol, 0 = off    */
+    int residual_every;           /* steps between residual evaluations (>= 1)       */
+    long long max_steps;
+    int steps_per_graph;          /* steps captured per CUDA graph launch (0 = auto) */
+} mpd_run_params;
+
+typedef struct mpd_run_stats {
+    long long steps;     /* steps taken by this call            */
+    double t;            /* simulated time reached              */
+    double dt;           /* next dt                             */
+    double residual;     /* last L-inf residual evaluated       */
+    double change;       /* last relative-L2 change evaluated   */
+    double max_wave_speed;
+    int converged;       /* 1 = residual or change criterion met */
+    int status;          /* MPD_OK or MPD_ERR_NONFINITE          */
+    double device_ms;    /* device time of the loop (CUDA events) */
+} mpd_run_stats;
+
+int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats);
+
+/* ---- diagnostics (each waits for the stream) ----------------------------- */
+/* Diagnostics::MaxWaveSpeed, src/diagnostics.cpp:14-43 */
+int mpd_max_wave_speed(mpd_solver *s, double *out);
+/* Diagnostics::ComputeDt, src/diagnostics.cpp:49-65 */
+int mpd_compute_dt(mpd_solver *s, double cfl_number, double growth, double dt_min,
+                   double dt_max, double dt_current, double *dt_next);
+/* Diagnostics::SolutionChange, src/diagnostics.cpp:71-106 (needs with_prev) */
+int mpd_solution_change(mpd_solver *s, double *out);
+/* Fields::SavePrev, src/fields.cpp:59-74 */
+int mpd_save_prev(mpd_solver *s);
+/* Verification::ComputeIntegrals, src/verification.cpp:16-45:
+ * mass, mom_z, mom_r, mom_phi, energy, mag_flux_z, mag_flux_phi */
+int mpd_integrals(mpd_solver *s, double out7[7]);
+/* Diagnostics::GetMassFlux / GetThrust, src/integrals.cpp:45-112 */
+int mpd_outlet(mpd_solver *s, double *mass_flux, double *thrust);
+/* Verification::CheckRadialSymmetry, src/verification.cpp:121-146 */
+int mpd_radial_symmetry(mpd_solver *s, double *out);
+/* The L-inf residual of the last step (new; no reference counterpart):
+ * max_k |u_k^{n+1} - u_k^n|_inf / max(|u_k^n|_inf, 1e-300) over interior cells. */
+int mpd_residual(mpd_solver *s, double *out);
+/* Physical values at one interior cell (the probe of src/main.cpp:258-275):
+ * out10 in MPD_RHO..MPD_H_PHI order, l_global in [0,L_max-1], m_global in [0,M_max]. */
+int mpd_probe(mpd_solver *s, int l_global, int m_global, double out10[10]);
+/* Simulated time and step count of the handle. */
+int mpd_time(mpd_solver *s, double *t, long long *step);
+
+/* ---- state transfer --------------------------------------------------------- */
+/* which: 0..7 conserved u0_1..u0_8, 8..17 physical planes MPD_RHO..MPD_H_PHI
+ * (the reference's Fields arrays after the step).  Copies one dense plane into
+ * host memory and waits. */
+int mpd_download(mpd_solver *s, int which, double *host_plane);
+/* Snapshot for I/O (IOManager::WriteFrame, src/io_manager.cpp:68-77): enqueue a
+ * copy of all 10 physical planes into caller-owned PINNED host memory
+ * (10 dense planes) on a side stream and return at once; mpd_snapshot_wait
+ * blocks until that copy has landed.  Stepping may continue meanwhile. */
+int mpd_snapshot_async(mpd_solver *s, double *pinned_phys10);
+int mpd_snapshot_wait(mpd_solver *s);
+/* Replace the state by new physical planes (restart; IInitialCondition::Apply
+ * + Fields::InitConservative).  Resets step and time to 0. */
+int mpd_set_physical(mpd_solver *s, const double *phys10);
+
+/* The handle's CUDA stream (a cudaStream_t), for callers that time or order
+ * work around the solver. */
+int mpd_get_stream(mpd_solver *s, void **stream);
+/* Bytes of device memory the handle holds. */
+int mpd_device_bytes(mpd_solver *s, size_t *bytes);
+
+/* Measurement support (new; no reference counterpart): advance `steps` steps
+ * with time step dt, launching eagerly with CUDA events around each kernel on
+ * the handle's stream, and return the mean device time per launch in ms of
+ * the interior kernel (out_ms[0]) and the boundary kernel (out_ms[1]). */
+int mpd_profile_kernels(mpd_solver *s, int steps, double dt, double out_ms[2]);
+
+/* ---- host-side expression initial condition ---------------------------------- */
+/* ExpressionIC::Apply, src/ics/expression_ic.cpp:286-324, evaluated on the host
+ * with the library's expression compiler.  exprs: 8 strings in the
+ * evaluation order rho, v_z, v_r, v_phi, H_z, H_r, H_phi, e (NULL entries take
+ * the reference defaults of src/ics/expression_ic.cpp:263-270); user constants
+ * as parallel name/value arrays.  Writes 10 dense physical planes. */
+int mpd_expression_ic(const mpd_config *cfg, const mpd_geometry *geom,
+                      const char *const exprs[8], int n_vars, const char *const *var_names,
+                      const double *var_values, double *phys10_out);
+
+/* Compile and evaluate one expression over named scalars (host).  Used by the
+ * config front end to validate expressions early. */
+int mpd_eval_expression(const char *src, int n_syms, const char *const *names,
+                        const double *values, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPD_B200_H */

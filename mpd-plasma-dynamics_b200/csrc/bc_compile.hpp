@@ -1,0 +1,34 @@
+// Host-side compilation of the boundary configuration into the flat table the
+// boundary kernel reads: FaceBC::FromConfig + PerFieldBC's constructor
+// (src/face_bc.cpp:23-36, src/bcs/per_field_bc.cpp:188-243) plus the range
+// resolution of FaceBC::Apply for a single rank that owns every face
+// (src/face_bc.cpp:56-129).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/mpd_b200.h"
+#include "lf_core.cuh"
+
+namespace mpd {
+
+struct CompiledBc {
+    int nseg[4] = {0, 0, 0, 0};
+    int first[4] = {0, 0, 0, 0};
+    std::vector<SegDesc> seg;
+    std::vector<int32_t> code;
+    std::vector<double> consts;
+};
+
+// Boundary expression symbol names in BcSym order.
+const std::vector<std::string> &BcSymbolNames();
+
+// Returns an MPD_* status; on failure `err` holds a message in the
+// reference's wording where the reference has one.
+int CompileBc(const mpd_config &cfg, CompiledBc &out, std::string &err);
+
+// Checks the grid sizes and pointers of a configuration (MPD_OK or MPD_ERR_INVALID).
+int ValidateConfig(const mpd_config *cfg, const mpd_geometry *geom, std::string &err);
+
+}  // namespace mpd

@@ -1,0 +1,533 @@
+// CUDA kernels of the plain FP64 path (everything except the fast interior
+// kernel, which lives in lf_fast.cuh).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <float.h>
+
+#include "lf_core.cuh"
+
+namespace mpd {
+
+// Device-resident controller and reduction accumulators of one solve.  The
+// boundary kernel's last block finalises each step here, so a captured CUDA
+// graph can run many steps without the host (dt, t, step, stop flags stay on
+// the device).
+struct DevState {
+    double t, dt, dt_used, T;
+    long long step, max_steps;
+    int done, converged, run_mode, adaptive;
+    double cfl, growth, dt_min, dt_max;
+    double resid_tol;
+    int resid_every, want_ws;
+    double conv_thr;
+    int check_freq, check_due;
+    double last_ws, last_resid, last_change;
+    int ws_valid, nonfinite, resid_valid, pad1;
+    unsigned long long ws_acc;
+    unsigned long long num_acc[8], den_acc[8];
+    unsigned int nf_acc, arrive;
+    double snap[16];
+};
+
+constexpr int kFlagWs = 1;
+constexpr int kFlagRes = 2;
+
+__device__ __forceinline__ int step_flags(const DevState *st) {
+    int f = 0;
+    if (st->want_ws) f |= kFlagWs;
+    if (st->resid_every > 0 && ((st->step + 1) % st->resid_every) == 0) f |= kFlagRes;
+    return f;
+}
+
+// Non-negative double as an order-preserving 64-bit key; NaN reported as 0
+// and flagged.
+__device__ __forceinline__ unsigned long long max_key(double x, unsigned int &nf) {
+    if (!(x == x)) {
+        nf = 1u;
+        return 0ull;
+    }
+    return (unsigned long long)__double_as_longlong(x > 0.0 ? x : 0.0);
+}
+
+// Block-wide max of NV keys (any block size <= 1024, multiple of 32) followed
+// by one atomicMax per key; also ORs the non-finite flag.
+template <int NV>
+__device__ __forceinline__ void block_max_atomic(unsigned long long (&key)[NV], unsigned int nf,
+                                                 unsigned long long *dst[NV], unsigned int *nf_dst) {
+    __shared__ unsigned long long red[32][NV];
+    __shared__ unsigned int nf_red[32];
+    const int lane = threadIdx.x & 31;
+    const int warp = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
+    const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        unsigned long long v = key[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = w > v ? w : v;
+        }
+        key[k] = v;
+    }
+    nf = __any_sync(0xffffffffu, nf != 0u) ? 1u : 0u;
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) red[warp][k] = key[k];
+        nf_red[warp] = nf;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            unsigned long long v = lane < nwarps ? red[lane][k] : 0ull;
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+                v = w > v ? w : v;
+            }
+            if (lane == 0 && dst[k] && v) atomicMax(dst[k], v);
+        }
+        unsigned int f = lane < nwarps ? nf_red[lane] : 0u;
+        f = __any_sync(0xffffffffu, f != 0u) ? 1u : 0u;
+        if (lane == 0 && f) atomicOr(nf_dst, 1u);
+    }
+}
+
+// Accumulate the wave speed and residual contributions of a finished cell.
+struct CellStats {
+    unsigned long long key[17];  // 0: wave speed, 1..8: |du|, 9..16: |u0|
+    unsigned int nf;
+    __device__ __forceinline__ void init() {
+#pragma unroll
+        for (int k = 0; k < 17; ++k) key[k] = 0ull;
+        nf = 0u;
+    }
+    __device__ __forceinline__ void add_ws(double s) {
+        if (!isfinite(s)) nf = 1u;
+        const unsigned long long k = max_key(s, nf);
+        key[0] = k > key[0] ? k : key[0];
+    }
+    __device__ __forceinline__ void add_res(const double *un, const double *uo) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const unsigned long long a = max_key(fabs(un[k] - uo[k]), nf);
+            const unsigned long long b = max_key(fabs(uo[k]), nf);
+            key[1 + k] = a > key[1 + k] ? a : key[1 + k];
+            key[9 + k] = b > key[9 + k] ? b : key[9 + k];
+        }
+    }
+    __device__ __forceinline__ void flush(DevState *st, int flags) {
+        unsigned long long *dst[17];
+        dst[0] = (flags & kFlagWs) ? &st->ws_acc : nullptr;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            dst[1 + k] = (flags & kFlagRes) ? &st->num_acc[k] : nullptr;
+            dst[9 + k] = (flags & kFlagRes) ? &st->den_acc[k] : nullptr;
+        }
+        block_max_atomic<17>(key, nf, dst, &st->nf_acc);
+    }
+};
+
+// Exact interior update (Solver::ComputeCentralUpdate + the implicit
+// UpdatePhysicalFromU of the neighbours), one thread per cell
+// l in [1, L], m in [2, M].  FIRST: the stencil reads the initial physical
+// planes instead of reconstructing them (step 0 of src/main.cpp:147-148).
+template <bool FIRST>
+__global__ void __launch_bounds__(256) lf_exact_kernel(Geo g, double *buf0, double *buf1,
+                                                       const double *__restrict__ ic, DevState *st,
+                                                       double dt_arg, int use_state_dt) {
+    if (st->done) return;
+    const long long step = st->step;
+    const double *__restrict__ u0 = (step & 1) ? buf1 : buf0;
+    double *__restrict__ u = (step & 1) ? buf0 : buf1;
+    const double dt = use_state_dt ? st->dt : dt_arg;
+    const int flags = step_flags(st);
+    const int m = 2 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int l = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    CellStats cs;
+    cs.init();
+    if (m <= g.M && l <= g.L) {
+        double U[5][8];
+        Phys Q[5];
+        double R[5];
+        const int ls[5] = {l, l + 1, l - 1, l, l};
+        const int ms[5] = {m, m, m, m + 1, m - 1};
+#pragma unroll
+        for (int p = 0; p < 5; ++p) {
+            const size_t i = g.ix(ls[p], ms[p]);
+            R[p] = g.r(ls[p], ms[p]);
+            load_cons(u0, g.ps, i, U[p]);
+            if (ls[p] == 0 || ls[p] == g.L + 1) Q[p] = phys_zero();
+            else if (FIRST) Q[p] = load_phys(ic, g.ps, i);
+            else Q[p] = recon_exact(U[p], R[p], g.gamma);
+        }
+        double out[8];
+        lf_cell_exact(U, Q, R, dt, g.dz, g.dr[l], out);
+        const size_t ic0 = g.ix(l, m);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) u[(size_t)k * g.ps + ic0] = out[k];
+        if (m == g.M && (l == 1 || l == g.L)) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) st->snap[(l == 1 ? 0 : 8) + k] = out[k];
+        }
+        if (l >= 2 && l <= g.L - 1) {  // cells no boundary face can overwrite
+            if (flags & kFlagWs) cs.add_ws(wave_speed(recon_exact(out, R[0], g.gamma), g.gamma));
+            if (flags & kFlagRes) cs.add_res(out, U[0]);
+        }
+    }
+    if (flags) cs.flush(st, flags);
+}
+
+// Boundary faces, one thread per boundary-ring cell, plus the end-of-step
+// controller in the last block to finish.
+__global__ void __launch_bounds__(128) bc_kernel(Geo g, double *buf0, double *buf1,
+                                                 const double *__restrict__ ic, BcTable bc,
+                                                 DevState *st, double dt_arg, int use_state_dt) {
+    if (st->done) return;
+    const long long step = st->step;
+    const double *u0 = (step & 1) ? buf1 : buf0;
+    double *u = (step & 1) ? buf0 : buf1;
+    const double dt = use_state_dt ? st->dt : dt_arg;
+    const int flags = step_flags(st);
+    BcView v;
+    v.g = g;
+    v.u0 = u0;
+    v.u = u;
+    v.ic = ic;
+    v.snap = st->snap;
+    v.first = step == 0;
+    v.dt = dt;
+    v.bc = bc;
+    CellStats cs;
+    cs.init();
+    const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i < ring_count(g)) {
+        int l, m;
+        ring_cell(g, i, l, m);
+        double uf[8];
+        bc_ring_final(v, l, m, uf);
+        const size_t ix = g.ix(l, m);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) u[(size_t)k * g.ps + ix] = uf[k];
+        if (flags & kFlagWs) cs.add_ws(wave_speed(recon_exact(uf, g.r(l, m), g.gamma), g.gamma));
+        if (flags & kFlagRes) {
+            double uo[8];
+            load_cons(u0, g.ps, ix, uo);
+            cs.add_res(uf, uo);
+        }
+    }
+    cs.flush(st, flags);
+
+    // ---- last block: finalise the step -------------------------------------
+    __shared__ int is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(&st->arrive, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!is_last || threadIdx.x != 0) return;
+    __threadfence();
+    volatile DevState *vs = st;
+    double ws = 0.0;
+    if (flags & kFlagWs) {
+        ws = __longlong_as_double((long long)vs->ws_acc);
+        vs->last_ws = ws;
+        vs->ws_valid = 1;
+    } else {
+        vs->ws_valid = 0;
+    }
+    double R = 0.0;
+    if (flags & kFlagRes) {
+        for (int k = 0; k < 8; ++k) {
+            const double num = __longlong_as_double((long long)vs->num_acc[k]);
+            const double den = __longlong_as_double((long long)vs->den_acc[k]);
+            const double q = num / (den > 1e-300 ? den : 1e-300);
+            R = q > R ? q : R;
+        }
+        vs->last_resid = R;
+        vs->resid_valid = 1;
+    }
+    if (vs->nf_acc || !isfinite(R) || !isfinite(ws)) vs->nonfinite = 1;
+    const double t = vs->t + dt;
+    const long long nstep = step + 1;
+    vs->t = t;
+    vs->dt_used = dt;
+    vs->step = nstep;
+    if (vs->run_mode) {
+        double dtn = dt;
+        if (vs->adaptive)
+            dtn = compute_dt_from_speed(ws, g.dz, g.dy, vs->cfl, vs->growth, vs->dt_min, vs->dt_max, dt);
+        int done = 0;
+        if ((flags & kFlagRes) && vs->resid_tol > 0.0 && R <= vs->resid_tol) {
+            vs->converged = 1;
+            done = 1;
+        }
+        if (vs->nonfinite || !(t < vs->T) || nstep >= vs->max_steps) done = 1;
+        if (t + dtn > vs->T) dtn = vs->T - t;
+        vs->dt = dtn;
+        vs->check_due = (vs->conv_thr > 0.0 && vs->check_freq > 0 && nstep % vs->check_freq == 0);
+        vs->done = done;
+    }
+    vs->ws_acc = 0ull;
+    for (int k = 0; k < 8; ++k) {
+        vs->num_acc[k] = 0ull;
+        vs->den_acc[k] = 0ull;
+    }
+    vs->nf_acc = 0u;
+    __threadfence();
+    vs->arrive = 0u;
+}
+
+// ---------------------------------------------------------------------------
+// Reductions over the current state (Diagnostics / Verification).
+// The current physical state is the initial condition before the first step,
+// otherwise UpdatePhysicalFromU of the current conserved planes.
+// ---------------------------------------------------------------------------
+struct StateView {
+    Geo g;
+    const double *u0;
+    const double *ic;
+    int first;
+    __device__ __forceinline__ Phys phys(int l, int m) const {
+        const size_t i = g.ix(l, m);
+        if (first) return load_phys(ic, g.ps, i);
+        double u[8];
+        load_cons(u0, g.ps, i, u);
+        return recon_exact(u, g.r(l, m), g.gamma);
+    }
+};
+
+// The current state's view, chosen on the device from the step counter so
+// that the same launch works inside captured graphs.
+struct StateBufs {
+    Geo g;
+    const double *buf0, *buf1, *ic;
+    const DevState *st;
+    __device__ __forceinline__ StateView view() const {
+        StateView sv;
+        sv.g = g;
+        const long long step = st->step;
+        sv.u0 = (step & 1) ? buf1 : buf0;
+        sv.ic = ic;
+        sv.first = step == 0;
+        return sv;
+    }
+};
+
+// Diagnostics::MaxWaveSpeed over [1,L] x [1,M+1] (max is order-free: exact).
+__global__ void wave_speed_kernel(StateBufs sb, unsigned long long *out) {
+    const StateView sv = sb.view();
+    unsigned long long key[1] = {0ull};
+    unsigned int nf = 0u;
+    const int total = sv.g.L * (sv.g.M + 1);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int l = 1 + i / (sv.g.M + 1), m = 1 + i % (sv.g.M + 1);
+        const double s = wave_speed(sv.phys(l, m), sv.g.gamma);
+        // std::max(local_max, s): NaN never replaces the running max
+        if (s == s) {
+            const unsigned long long k = max_key(s, nf);
+            key[0] = k > key[0] ? k : key[0];
+        }
+    }
+    unsigned long long *dst[1] = {out};
+    block_max_atomic<1>(key, nf, dst, reinterpret_cast<unsigned int *>(out + 1));
+}
+
+// Verification::CheckRadialSymmetry (src/verification.cpp:121-146).
+__global__ void radial_kernel(StateBufs sb, unsigned long long *out) {
+    const StateView sv = sb.view();
+    unsigned long long key[1] = {0ull};
+    unsigned int nf = 0u;
+    const int W = sv.g.M;  // m = 1..M (pairs m, m+1)
+    const int total = sv.g.L * W;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int l = 1 + i / W, m = 1 + i % W;
+        const double a = sv.phys(l, m).rho;
+        const double b = sv.phys(l, m + 1).rho;
+        const double mean = 0.5 * (a + b);
+        if (mean > 1.0e-15) {
+            const double q = fabs(b - a) / mean;
+            if (q == q) {
+                const unsigned long long k = max_key(q, nf);
+                key[0] = k > key[0] ? k : key[0];
+            }
+        }
+    }
+    unsigned long long *dst[1] = {out};
+    block_max_atomic<1>(key, nf, dst, reinterpret_cast<unsigned int *>(out + 1));
+}
+
+// Deterministic block sums: each block writes NV partial sums for its rows,
+// a single-block pass adds the partials in block order.
+template <int NV>
+__device__ __forceinline__ void block_sum_store(double (&v)[NV], double *partials) {
+    __shared__ double red[32][NV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) red[warp][k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < NV; ++k) {
+            double s = 0.0;
+            for (int w = 0; w < nwarps; ++w) s += red[w][k];
+            partials[(size_t)blockIdx.x * NV + k] = s;
+        }
+    }
+}
+
+template <int NV>
+__global__ void sum_partials_kernel(const double *partials, int nblocks, double *out) {
+    if (threadIdx.x >= NV) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partials[(size_t)b * NV + threadIdx.x];
+    out[threadIdx.x] = s;
+}
+
+// Verification::ComputeIntegrals (src/verification.cpp:16-45): block b sums
+// rows l = 1 + b, 1 + b + gridDim.x, ... in m order.  Output order:
+// mass, mom_z, mom_r, mom_phi, energy, mag_flux_z (u_7), mag_flux_phi (u_6).
+__global__ void integrals_kernel(StateBufs sb, double *partials) {
+    const StateView sv = sb.view();
+    const Geo &g = sv.g;
+    const double *u0 = sv.u0;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int l = 1 + blockIdx.x; l <= g.L; l += gridDim.x) {
+        const double cell_area = g.dr[l] * g.dz;
+        for (int m = 1 + threadIdx.x; m <= g.M + 1; m += blockDim.x) {
+            const size_t i = g.ix(l, m);
+            acc[0] += u0[0 * g.ps + i] * cell_area;
+            acc[1] += u0[1 * g.ps + i] * cell_area;
+            acc[2] += u0[2 * g.ps + i] * cell_area;
+            acc[3] += u0[3 * g.ps + i] * cell_area;
+            acc[4] += u0[4 * g.ps + i] * cell_area;
+            acc[5] += u0[6 * g.ps + i] * cell_area;
+            acc[6] += u0[5 * g.ps + i] * cell_area;
+        }
+    }
+    block_sum_store<7>(acc, partials);
+}
+
+// Diagnostics::SolutionChange + Fields::SavePrev (src/diagnostics.cpp:71-106,
+// src/fields.cpp:59-74): sums of squared differences against the prev planes
+// and of squared values, then prev <- current.
+__global__ void change_kernel(StateBufs sb, double *prev, double *partials, int save,
+                              int only_if_due) {
+    if (only_if_due && !sb.st->check_due) return;
+    const StateView sv = sb.view();
+    double acc[2] = {0.0, 0.0};
+    const Geo &g = sv.g;
+    for (int l = 1 + blockIdx.x; l <= g.L; l += gridDim.x) {
+        for (int m = 1 + threadIdx.x; m <= g.M + 1; m += blockDim.x) {
+            const size_t i = g.ix(l, m);
+            const Phys q = sv.phys(l, m);
+            const double x[7] = {q.rho, q.vz, q.vr, q.vphi, q.Hz, q.Hr, q.Hphi};
+            double d[7];
+#pragma unroll
+            for (int k = 0; k < 7; ++k) d[k] = x[k] - prev[(size_t)k * g.ps + i];
+            acc[0] += d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + d[3] * d[3] + d[4] * d[4]
+                    + d[5] * d[5] + d[6] * d[6];
+            acc[1] += x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3] + x[4] * x[4]
+                    + x[5] * x[5] + x[6] * x[6];
+            if (save) {
+#pragma unroll
+                for (int k = 0; k < 7; ++k) prev[(size_t)k * g.ps + i] = x[k];
+            }
+        }
+    }
+    block_sum_store<2>(acc, partials);
+}
+
+// Final relative change and the run loop's convergence decision
+// (src/main.cpp:233-247).  Runs as one thread after change_kernel.
+__global__ void change_finish_kernel(const double *partials, int nblocks, DevState *st,
+                                     int from_run) {
+    if (threadIdx.x != 0) return;
+    if (from_run && !st->check_due) return;
+    double sd = 0.0, sc = 0.0;
+    for (int b = 0; b < nblocks; ++b) {
+        sd += partials[2 * b];
+        sc += partials[2 * b + 1];
+    }
+    const double nd = sqrt(sd), nc = sqrt(sc);
+    const double change = (nc > 1e-15) ? (nd / nc) : nd;
+    st->last_change = change;
+    if (from_run) {
+        st->check_due = 0;
+        if (change < st->conv_thr) {
+            st->converged = 1;
+            st->done = 1;
+        }
+    }
+}
+
+// Diagnostics::GetMassFlux / GetThrust (src/integrals.cpp:45-112): the outlet
+// column is summed serially in m order by one thread, as the reference does.
+__global__ void outlet_kernel(StateBufs sb, double inv_8pi, double *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const StateView sv = sb.view();
+    const Geo &g = sv.g;
+    const int l = g.L;
+    const double dr_out = g.dr[l];
+    double sm = 0.0, sth = 0.0;
+    for (int m_local = 1; m_local <= g.M + 1; ++m_local) {
+        const int m_global = m_local - 1;
+        const double w = (m_global == 0 || m_global == g.M) ? 0.5 : 1.0;
+        const Phys q = sv.phys(l, m_local);
+        const double r = g.r(l, m_local);
+        const double fm = q.rho * q.vz;
+        const double Fm = fm * 2.0 * M_PI * r;
+        sm += w * Fm * dr_out;
+        const double v_z2 = q.vz * q.vz;
+        const double H2 = q.Hz * q.Hz + q.Hr * q.Hr + q.Hphi * q.Hphi;
+        const double ft = q.rho * v_z2 + q.p + H2 * inv_8pi;
+        const double Ft = ft * 2.0 * M_PI * r;
+        sth += w * Ft * dr_out;
+    }
+    out[0] = sm;
+    out[1] = sth;
+}
+
+// Materialise the 10 physical planes of the current state (pitched); ghost
+// cells are zero as in the reference's Fields arrays.
+__global__ void phys_planes_kernel(StateBufs sb, double *out) {
+    const StateView sv = sb.view();
+    const Geo &g = sv.g;
+    const int cols = g.M + 3, rows = g.L + 2;
+    const int total = rows * cols;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int l = i / cols, m = i % cols;
+        Phys q = phys_zero();
+        if (l >= 1 && l <= g.L && m >= 1 && m <= g.M + 1) q = sv.phys(l, m);
+        const size_t o = g.ix(l, m);
+        out[0 * g.ps + o] = q.rho;
+        out[1 * g.ps + o] = q.vz;
+        out[2 * g.ps + o] = q.vr;
+        out[3 * g.ps + o] = q.vphi;
+        out[4 * g.ps + o] = q.e;
+        out[5 * g.ps + o] = q.p;
+        out[6 * g.ps + o] = q.P;
+        out[7 * g.ps + o] = q.Hz;
+        out[8 * g.ps + o] = q.Hr;
+        out[9 * g.ps + o] = q.Hphi;
+    }
+}
+
+// Fields::InitConservative (src/fields.cpp:40-57) on the device: interior
+// cells from the physical planes, ghosts zero.
+__global__ void init_conservative_kernel(Geo g, const double *ic, double *u0) {
+    const int cols = g.M + 3, rows = g.L + 2;
+    const int total = rows * cols;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int l = i / cols, m = i % cols;
+        const size_t o = g.ix(l, m);
+        double u[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (l >= 1 && l <= g.L && m >= 1 && m <= g.M + 1) rebuild_u(load_phys(ic, g.ps, o), g.r(l, m), u);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) u0[(size_t)k * g.ps + o] = u[k];
+    }
+}
+
+}  // namespace mpd

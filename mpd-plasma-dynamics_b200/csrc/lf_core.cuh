@@ -1,0 +1,788 @@
+// Core per-cell arithmetic of the Lax-Friedrichs hot path.
+//
+// Every function here is host+device (MPD_HD) so that the exact same source
+// runs inside the CUDA kernels and inside the host emulator that the CPU test
+// suite drives.  The whole library is compiled with --fmad=false /
+// -ffp-contract=off: in the "exact" functions each expression is one IEEE-754
+// operation per operator, in the reference's operand order, with true
+// divides, which makes them bit-identical to the reference.  The "fast"
+// interior kernel (lf_fast.cuh) opts into FMA explicitly.
+//
+// Storage: conserved planes u_1..u_8 in structure-of-arrays layout, plane k
+// at base + k*ps, cell (l, m) at l*pitch + m; the reference's (L+2)x(M+3)
+// index space with one ghost layer (single rank: ghosts stay zero).
+#pragma once
+
+#include <math.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define MPD_HD __host__ __device__ __forceinline__
+#else
+#define MPD_HD inline
+#endif
+
+#include "expr_ops.h"
+
+namespace mpd {
+
+constexpr int kNumCons = 8;
+constexpr int kNumPhys = 10;
+constexpr int kMaxSegments = 32;  // all faces together
+
+// Physical plane order = Fields members (include/fields.hpp:35-37).
+enum PhysIdx { P_RHO = 0, P_VZ, P_VR, P_VPHI, P_E, P_PG, P_PT, P_HZ, P_HR, P_HPHI };
+// Boundary field evaluation order (src/bcs/per_field_bc.cpp:319-362):
+// rho, v_z, v_r, v_phi, H_z, H_r, H_phi, e.
+enum PrimIdx { Q_RHO = 0, Q_VZ, Q_VR, Q_VPHI, Q_HZ, Q_HR, Q_HPHI, Q_E };
+enum FaceIdx { FACE_L_LO = 0, FACE_L_HI = 1, FACE_M_LO = 2, FACE_M_HI = 3 };
+enum CondType { COND_NEUMANN = 0, COND_DIRICHLET = 1, COND_EXPR = 2, COND_AXIS_LF = 3 };
+
+// Boundary expression symbols (PerFieldBC::ExprImpl, src/bcs/per_field_bc.cpp:81-119).
+enum BcSym {
+    BS_GAMMA = 0, BS_BETA, BS_HZ0, BS_R0, BS_DZ, BS_DR, BS_R, BS_RZ, BS_Z, BS_RNB, BS_RZNB,
+    BS_NB0,            // rho_nb, v_z_nb, v_r_nb, v_phi_nb, e_nb, H_z_nb, H_r_nb, H_phi_nb
+    BS_CUR0 = BS_NB0 + 8,  // rho, v_z, v_r, v_phi, H_z, H_r, H_phi, e (evaluation order)
+    BS_COUNT = BS_CUR0 + 8
+};
+
+struct Phys {
+    double rho, vz, vr, vphi, e, p, P, Hz, Hr, Hphi;
+};
+
+// Grid geometry: Grid::Build (src/grid.cpp:20-42) recomputed on the fly from
+// the wall profiles, so no r plane is stored.
+struct Geo {
+    int L, M, pitch;
+    size_t ps;  // plane stride (doubles)
+    double dz, dy, gamma, beta, H_z0, r_0;
+    const double *rin, *rout, *drin, *drout, *dr;  // per row l = 0..L+1
+
+    MPD_HD size_t ix(int l, int m) const { return (size_t)l * (size_t)pitch + (size_t)m; }
+    MPD_HD double r(int l, int m) const {
+        const double frac = (double)(m - 1) * dy;
+        return (1.0 - frac) * rin[l] + frac * rout[l];
+    }
+    MPD_HD double rz(int l, int m) const {
+        const double frac = (double)(m - 1) * dy;
+        return (1.0 - frac) * drin[l] + frac * drout[l];
+    }
+};
+
+MPD_HD void load_cons(const double *base, size_t ps, size_t i, double u[8]) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) u[k] = base[(size_t)k * ps + i];
+}
+
+// Fields::UpdatePhysicalFromU (src/fields.cpp:76-99), one cell.
+MPD_HD Phys recon_exact(const double u[8], double r, double gamma) {
+    Phys q;
+    q.rho = u[0] / r;
+    q.vz = u[1] / u[0];
+    q.vr = u[2] / u[0];
+    q.vphi = u[3] / u[0];
+    q.Hphi = u[5];
+    q.Hz = u[6] / r;
+    q.Hr = u[7] / r;
+    q.e = u[4] / u[0];
+    q.p = (gamma - 1.0) * q.rho * q.e;
+    q.P = q.p + 0.5 * (q.Hz * q.Hz + q.Hr * q.Hr + q.Hphi * q.Hphi);
+    return q;
+}
+
+MPD_HD Phys phys_zero() {
+    Phys q;
+    q.rho = q.vz = q.vr = q.vphi = q.e = q.p = q.P = q.Hz = q.Hr = q.Hphi = 0.0;
+    return q;
+}
+
+MPD_HD Phys load_phys(const double *base, size_t ps, size_t i) {
+    Phys q;
+    q.rho = base[0 * ps + i];
+    q.vz = base[1 * ps + i];
+    q.vr = base[2 * ps + i];
+    q.vphi = base[3 * ps + i];
+    q.e = base[4 * ps + i];
+    q.p = base[5 * ps + i];
+    q.P = base[6 * ps + i];
+    q.Hz = base[7 * ps + i];
+    q.Hr = base[8 * ps + i];
+    q.Hphi = base[9 * ps + i];
+    return q;
+}
+
+// include/physics_utils.hpp:15-24 (RebuildUFromPhysical), one cell.
+MPD_HD void rebuild_u(const Phys &q, double r, double u[8]) {
+    u[0] = q.rho * r;
+    u[1] = q.rho * q.vz * r;
+    u[2] = q.rho * q.vr * r;
+    u[3] = q.rho * q.vphi * r;
+    u[4] = q.rho * q.e * r;
+    u[5] = q.Hphi;
+    u[6] = q.Hz * r;
+    u[7] = q.Hr * r;
+}
+
+// One term of Diagnostics::MaxWaveSpeed (src/diagnostics.cpp:25-35).
+MPD_HD double wave_speed(const Phys &q, double gamma) {
+    const double cs = sqrt(gamma * q.p / q.rho);
+    const double ca = sqrt((q.Hz * q.Hz + q.Hr * q.Hr + q.Hphi * q.Hphi) / q.rho);
+    const double v = sqrt(q.vz * q.vz + q.vr * q.vr);
+    return v + cs + ca;
+}
+
+// Diagnostics::ComputeDt clamp arithmetic (src/diagnostics.cpp:57-64) with
+// std::min / std::clamp comparison semantics.
+MPD_HD double compute_dt_from_speed(double speed, double dz, double dy, double cfl,
+                                    double growth, double dt_min, double dt_max,
+                                    double dt_current) {
+    const double dx = (dy < dz) ? dy : dz;
+    const double dt_cfl = cfl * dx / (speed + 1.0e-10);
+    const double dt_grown = dt_current * growth;
+    const double v = (dt_grown < dt_cfl) ? dt_grown : dt_cfl;
+    return (v < dt_min) ? dt_min : ((dt_max < v) ? dt_max : v);
+}
+
+// ---------------------------------------------------------------------------
+// Solver::ComputeCentralUpdate (src/solver.cpp:59-153) for one cell, exact.
+// Stencil points: 0 = (l,m), 1 = (l+1,m), 2 = (l-1,m), 3 = (l,m+1), 4 = (l,m-1).
+// U[p][k] conserved u0 values, Q[p] physical values, R[p] radius.
+// ---------------------------------------------------------------------------
+MPD_HD void lf_cell_exact(const double U[5][8], const Phys Q[5], const double R[5], double dt,
+                          double dz, double dr_l, double out[8]) {
+    enum { C = 0, N = 1, S = 2, E = 3, W = 4 };
+#define UA(p) U[p][kk]
+    {
+        const int kk = 0;
+        out[0] = 0.25 * (UA(N) + UA(S) + UA(E) + UA(W))
+               + dt * (-(UA(N) * Q[N].vz - UA(S) * Q[S].vz) / (2 * dz)
+                       - (UA(E) * Q[E].vr - UA(W) * Q[W].vr) / (2 * dr_l));
+    }
+    {
+        const int kk = 1;
+        out[1] = 0.25 * (UA(N) + UA(S) + UA(E) + UA(W))
+               + dt * (((Q[N].Hz * Q[N].Hz - Q[N].P) * R[N] - (Q[S].Hz * Q[S].Hz - Q[S].P) * R[S]) / (2 * dz)
+                       + (Q[E].Hz * Q[E].Hr * R[E] - Q[W].Hz * Q[W].Hr * R[W]) / (2 * dr_l)
+                       - (UA(N) * Q[N].vz - UA(S) * Q[S].vz) / (2 * dz)
+                       - (UA(E) * Q[E].vr - UA(W) * Q[W].vr) / (2 * dr_l));
+    }
+    {
+        const int kk = 2;
+        out[2] = 0.25 * (UA(N) + UA(S) + UA(E) + UA(W))
+               + dt * ((Q[C].rho * Q[C].vphi * Q[C].vphi + Q[C].P - Q[C].Hphi * Q[C].Hphi)
+                       + (Q[N].Hz * Q[N].Hr * R[N] - Q[S].Hz * Q[S].Hr * R[S]) / (2 * dz)
+                       + ((Q[E].Hr * Q[E].Hr - Q[E].P) * R[E] - (Q[W].Hr * Q[W].Hr - Q[W].P) * R[W]) / (2 * dr_l)
+                       - (UA(N) * Q[N].vz - UA(S) * Q[S].vz) / (2 * dz)
+                       - (UA(E) * Q[E].vr - UA(W) * Q[W].vr) / (2 * dr_l));
+    }
+    {
+        const int kk = 3;
+        out[3] = 0.25 * (UA(N) + UA(S) + UA(E) + UA(W))
+               + dt * ((-Q[C].rho * Q[C].vr * Q[C].vphi + Q[C].Hphi * Q[C].Hr)
+                       + (Q[N].Hphi * Q[N].Hz * R[N] - Q[S].Hphi * Q[S].Hz * R[S]) / (2 * dz)
+                       + (Q[E].Hphi * Q[E].Hr * R[E] - Q[W].Hphi * Q[W].Hr * R[W]) / (2 * dr_l)
+                       - (UA(N) * Q[N].vz - UA(S) * Q[S].vz) / (2 * dz)
+                       - (UA(E) * Q[E].vr - UA(W) * Q[W].vr) / (2 * dr_l));
+    }
+    {
+        const int kk = 4;
+        out[4] = 0.25 * (UA(N) + UA(S) + UA(E) + UA(W))
+               + dt * (-Q[C].p * ((Q[N].vz * R[N] - Q[S].vz * R[S]) / (2 * dz)
+                                  + (Q[E].vr * R[E] - Q[W].vr * R[W]) / (2 * dr_l))
+                       - (UA(N) * Q[N].vz - UA(S) * Q[S].vz) / (2 * dz)
+                       - (UA(E) * Q[E].vr - UA(W) * Q[W].vr) / (2 * dr_l));
+    }
+    {
+        const int kk = 5;
+        out[5] = 0.25 * (UA(N) + UA(S) + UA(E) + UA(W))
+               + dt * ((Q[N].Hz * Q[N].vphi - Q[S].Hz * Q[S].vphi) / (2 * dz)
+                       + (Q[E].Hr * Q[E].vphi - Q[W].Hr * Q[W].vphi) / (2 * dr_l)
+                       - (UA(N) * Q[N].vz - UA(S) * Q[S].vz) / (2 * dz)
+                       - (UA(E) * Q[E].vr - UA(W) * Q[W].vr) / (2 * dr_l));
+    }
+    {
+        const int kk = 6;
+        out[6] = 0.25 * (UA(N) + UA(S) + UA(E) + UA(W))
+               + dt * ((Q[E].Hr * Q[E].vz * R[E] - Q[W].Hr * Q[W].vz * R[W]) / (2 * dr_l)
+                       - (UA(E) * Q[E].vr - UA(W) * Q[W].vr) / (2 * dr_l));
+    }
+    {
+        const int kk = 7;
+        out[7] = 0.25 * (UA(N) + UA(S) + UA(E) + UA(W))
+               + dt * ((Q[N].Hz * Q[N].vr * R[N] - Q[S].Hz * Q[S].vr * R[S]) / (2 * dz)
+                       - (UA(N) * Q[N].vz - UA(S) * Q[S].vz) / (2 * dz));
+    }
+#undef UA
+}
+
+// ---------------------------------------------------------------------------
+// Fast-mode point and cell arithmetic (MPD_PRECISION_FAST, lf_fast.cuh).
+// ---------------------------------------------------------------------------
+// Z-direction point quantities: conserved values and the z flux combination
+// of each equation (index 6, free because u_7 has no z flux, carries v_z r
+// for the -p div(r v) source of u_5).
+struct ZPoint {
+    double U[8];
+    double Gz[8];
+};
+// R-direction point quantities (index 7, free because u_8 has no r flux,
+// carries v_r r) and the cell-centred sources.
+struct RPoint {
+    double Gr[8];
+    double S3, S4, p;
+};
+
+MPD_HD void fast_point(const double U[8], double r, double gm1, ZPoint &z,
+                                           RPoint &q) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) z.U[k] = U[k];
+    const double ir = 1.0 / r;
+    const double iu = 1.0 / U[0];
+    const double rho = U[0] * ir;
+    const double vz = U[1] * iu, vr = U[2] * iu, vphi = U[3] * iu, e = U[4] * iu;
+    const double Hphi = U[5], Hz = U[6] * ir, Hr = U[7] * ir;
+    const double p = gm1 * rho * e;
+    const double P = fma(0.5, fma(Hz, Hz, fma(Hr, Hr, Hphi * Hphi)), p);
+    const double HzHr_r = Hz * Hr * r;
+    z.Gz[0] = -U[0] * vz;
+    z.Gz[1] = fma(fma(Hz, Hz, -P), r, -U[1] * vz);
+    z.Gz[2] = fma(-U[2], vz, HzHr_r);
+    z.Gz[3] = fma(Hphi * Hz, r, -U[3] * vz);
+    z.Gz[4] = -U[4] * vz;
+    z.Gz[5] = fma(Hz, vphi, -U[5] * vz);
+    z.Gz[6] = vz * r;
+    z.Gz[7] = fma(Hz * vr, r, -U[7] * vz);
+    q.Gr[0] = -U[0] * vr;
+    q.Gr[1] = fma(-U[1], vr, HzHr_r);
+    q.Gr[2] = fma(fma(Hr, Hr, -P), r, -U[2] * vr);
+    q.Gr[3] = fma(Hphi * Hr, r, -U[3] * vr);
+    q.Gr[4] = -U[4] * vr;
+    q.Gr[5] = fma(Hr, vphi, -U[5] * vr);
+    q.Gr[6] = fma(Hr * vz, r, -U[6] * vr);
+    q.Gr[7] = vr * r;
+    q.S3 = fma(rho * vphi, vphi, P) - Hphi * Hphi;
+    q.S4 = fma(-rho * vr, vphi, Hphi * Hr);
+    q.p = p;
+}
+
+MPD_HD void zero_point(ZPoint &z, RPoint &q) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        z.U[k] = 0.0;
+        z.Gz[k] = 0.0;
+        q.Gr[k] = 0.0;
+    }
+    q.S3 = q.S4 = q.p = 0.0;
+}
+
+// One cell of the fast update from its stencil's point quantities: S/N are
+// the z neighbours, C the cell itself, E/W the r neighbours' U and Gr.
+// kz = dt/(2 dz), kr = dt/(2 dr_l).
+MPD_HD void fast_cell(const ZPoint &zS, const ZPoint &zN, const RPoint &qC, const double Ue[8],
+                      const double Uw[8], const double Ge[8], const double Gw[8], double kz,
+                      double kr, double dt, double out[8]) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const double avg = 0.25 * ((zN.U[k] + zS.U[k]) + (Ue[k] + Uw[k]));
+        double v;
+        if (k == 6) {
+            v = fma(kr, Ge[6] - Gw[6], avg);               // u_7: r flux only
+        } else if (k == 7) {
+            v = fma(kz, zN.Gz[7] - zS.Gz[7], avg);         // u_8: z flux only
+        } else {
+            v = fma(kz, zN.Gz[k] - zS.Gz[k], fma(kr, Ge[k] - Gw[k], avg));
+            if (k == 2) v = fma(dt, qC.S3, v);
+            if (k == 3) v = fma(dt, qC.S4, v);
+        }
+        out[k] = v;
+    }
+    // u_5 source -p div(r v): index 6 of Gz carries v_z r, index 7 of Gr v_r r
+    const double div = fma(kz, zN.Gz[6] - zS.Gz[6], kr * (Ge[7] - Gw[7]));
+    out[4] = fma(-qC.p, div, out[4]);
+}
+
+// Wave speed of a new cell state in the fast kernel (reciprocals instead of
+// divides, IEEE sqrt).
+MPD_HD double fast_wave_speed(const double u[8], double r, double gamma) {
+    const double ir = 1.0 / r, iu = 1.0 / u[0];
+    const double rho = u[0] * ir, vz = u[1] * iu, vr = u[2] * iu;
+    const double e = u[4] * iu, Hphi = u[5], Hz = u[6] * ir, Hr = u[7] * ir;
+    const double prs = (gamma - 1.0) * rho * e;
+    const double irho = r * iu;
+    const double cs2 = gamma * prs * irho;
+    const double ca2 = fma(Hz, Hz, fma(Hr, Hr, Hphi * Hphi)) * irho;
+    const double v2 = fma(vz, vz, vr * vr);
+    return sqrt(v2) + sqrt(cs2) + sqrt(ca2);
+}
+
+// ---------------------------------------------------------------------------
+// Expression bytecode interpreter (codes from expr.cpp).
+// ---------------------------------------------------------------------------
+MPD_HD double eval_code(const int32_t *code, const double *consts, const double *sym) {
+    double st[kExprMaxStack];
+    int sp = 0;
+    for (int pc = 0;; ++pc) {
+        const int32_t ins = code[pc];
+        const int op = ins & 0xff;
+        const int arg = ins >> 8;
+        switch (op) {
+            case OP_END: return sp > 0 ? st[sp - 1] : 0.0;
+            case OP_CONST: st[sp++] = consts[arg]; break;
+            case OP_VAR: st[sp++] = sym[arg]; break;
+            case OP_NEG: st[sp - 1] = -st[sp - 1]; break;
+            case OP_ADD: st[sp - 2] = st[sp - 2] + st[sp - 1]; --sp; break;
+            case OP_SUB: st[sp - 2] = st[sp - 2] - st[sp - 1]; --sp; break;
+            case OP_MUL: st[sp - 2] = st[sp - 2] * st[sp - 1]; --sp; break;
+            case OP_DIV: st[sp - 2] = st[sp - 2] / st[sp - 1]; --sp; break;
+            case OP_MOD: st[sp - 2] = fmod(st[sp - 2], st[sp - 1]); --sp; break;
+            case OP_POW: st[sp - 2] = pow(st[sp - 2], st[sp - 1]); --sp; break;
+            case OP_ATAN2: st[sp - 2] = atan2(st[sp - 2], st[sp - 1]); --sp; break;
+            case OP_MIN2: {
+                const double y = st[sp - 1], x = st[sp - 2];
+                st[sp - 2] = y < x ? y : x;
+                --sp;
+                break;
+            }
+            case OP_MAX2: {
+                const double y = st[sp - 1], x = st[sp - 2];
+                st[sp - 2] = y > x ? y : x;
+                --sp;
+                break;
+            }
+            case OP_CLAMP: {
+                const double lo = st[sp - 3], v = st[sp - 2], hi = st[sp - 1];
+                st[sp - 3] = v < lo ? lo : (v > hi ? hi : v);
+                sp -= 2;
+                break;
+            }
+            case OP_FN1: {
+                const double x = st[sp - 1];
+                double y;
+                switch (arg) {
+                    case FN_SIN: y = sin(x); break;
+                    case FN_COS: y = cos(x); break;
+                    case FN_TAN: y = tan(x); break;
+                    case FN_ASIN: y = asin(x); break;
+                    case FN_ACOS: y = acos(x); break;
+                    case FN_ATAN: y = atan(x); break;
+                    case FN_EXP: y = exp(x); break;
+                    case FN_LOG: y = log(x); break;
+                    case FN_LOG2: y = log2(x); break;
+                    case FN_LOG10: y = log10(x); break;
+                    case FN_SQRT: y = sqrt(x); break;
+                    case FN_ABS: y = fabs(x); break;
+                    default: y = x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); break;
+                }
+                st[sp - 1] = y;
+                break;
+            }
+            default: return NAN;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Boundary conditions (FaceBC + PerFieldBC) for one boundary cell.
+// ---------------------------------------------------------------------------
+
+// One segment, compiled: local inclusive range along the face's free axis
+// after FaceBC::Apply's sentinel resolution, ClipToLocal and the M_LO corner
+// policy (src/face_bc.cpp:104-129); conditions in evaluation order.
+struct SegDesc {
+    int lo, hi;
+    int has_axis;
+    int pad;
+    int type[8];
+    int code[8];      // offset of the expression's bytecode, -1 if none
+    double value[8];
+};
+
+struct BcTable {
+    int nseg[4];
+    int first[4];             // index of the face's first segment in seg[]
+    const SegDesc *seg;
+    const int32_t *code;
+    const double *consts;
+};
+
+// Everything one boundary step reads.
+struct BcView {
+    Geo g;
+    const double *u0;    // conserved state at the start of the step
+    double *u;           // new state (interior written by the LF kernel)
+    const double *ic;    // initial physical planes (first step only)
+    const double *snap;  // central u of (1,M) [0..7] and (L,M) [8..15] before BCs
+    int first;           // step 0: "old" physical values are the IC planes
+    double dt;
+    BcTable bc;
+};
+
+// Primitive values in evaluation order.
+struct Prim {
+    double v[8];
+};
+
+MPD_HD Prim prim_of(const Phys &q) {
+    Prim p;
+    p.v[Q_RHO] = q.rho;
+    p.v[Q_VZ] = q.vz;
+    p.v[Q_VR] = q.vr;
+    p.v[Q_VPHI] = q.vphi;
+    p.v[Q_HZ] = q.Hz;
+    p.v[Q_HR] = q.Hr;
+    p.v[Q_HPHI] = q.Hphi;
+    p.v[Q_E] = q.e;
+    return p;
+}
+
+// Physical value of a cell as the previous step's full reconstruction left
+// it (or the initial condition on the first step).
+MPD_HD Phys old_phys(const BcView &v, int l, int m) {
+    const size_t i = v.g.ix(l, m);
+    if (v.first) return load_phys(v.ic, v.g.ps, i);
+    double u[8];
+    load_cons(v.u0, v.g.ps, i, u);
+    return recon_exact(u, v.g.r(l, m), v.g.gamma);
+}
+
+// Physical value of a central cell after this step's central update
+// (UpdateCentralPhysical, src/solver.cpp:155-159).
+MPD_HD Phys central_phys(const BcView &v, int l, int m) {
+    double u[8];
+    if (m == v.g.M && (l == 1 || l == v.g.L)) {
+        const double *s = v.snap + (l == 1 ? 0 : 8);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) u[k] = s[k];
+    } else {
+        load_cons(v.u, v.g.ps, v.g.ix(l, m), u);
+    }
+    return recon_exact(u, v.g.r(l, m), v.g.gamma);
+}
+
+// Last segment of `face` whose range covers free index k, or -1.
+MPD_HD int last_cover(const BcView &v, int face, int k, int limit) {
+    const int base = v.bc.first[face];
+    for (int s = limit; s >= 0; --s) {
+        const SegDesc &d = v.bc.seg[base + s];
+        if (k >= d.lo && k <= d.hi) return s;
+    }
+    return -1;
+}
+
+// PerFieldBC::Apply's per-cell field evaluation (src/bcs/per_field_bc.cpp:
+// 286-292 resolve, 311-360 / 393-446 expression path): writes the 8 new
+// primitives of cell (l, m) given its neighbour's primitives and the values
+// to keep (AxisLF fields keep the cell's current value).
+MPD_HD void eval_segment(const BcView &v, const SegDesc &d, int l, int m, int ln, int mn,
+                         const Prim &nb, const Prim &keep, Prim &out) {
+    double sym[BS_COUNT];
+    bool have_sym = false;
+    for (int j = 0; j < 8; ++j) {
+        double val;
+        switch (d.type[j]) {
+            case COND_NEUMANN: val = nb.v[j] + d.value[j]; break;
+            case COND_DIRICHLET: val = d.value[j]; break;
+            case COND_EXPR: {
+                if (!have_sym) {
+                    have_sym = true;
+                    sym[BS_GAMMA] = v.g.gamma;
+                    sym[BS_BETA] = v.g.beta;
+                    sym[BS_HZ0] = v.g.H_z0;
+                    sym[BS_R0] = v.g.r_0;
+                    sym[BS_DZ] = v.g.dz;
+                    sym[BS_DR] = v.g.dr[l];
+                    sym[BS_R] = v.g.r(l, m);
+                    sym[BS_RZ] = v.g.rz(l, m);
+                    sym[BS_Z] = (double)(l - 1) * v.g.dz;
+                    sym[BS_RNB] = v.g.r(ln, mn);
+                    sym[BS_RZNB] = v.g.rz(ln, mn);
+                    // *_nb symbols in the reference's SetNeighbors order:
+                    // rho, v_z, v_r, v_phi, e, H_z, H_r, H_phi
+                    sym[BS_NB0 + 0] = nb.v[Q_RHO];
+                    sym[BS_NB0 + 1] = nb.v[Q_VZ];
+                    sym[BS_NB0 + 2] = nb.v[Q_VR];
+                    sym[BS_NB0 + 3] = nb.v[Q_VPHI];
+                    sym[BS_NB0 + 4] = nb.v[Q_E];
+                    sym[BS_NB0 + 5] = nb.v[Q_HZ];
+                    sym[BS_NB0 + 6] = nb.v[Q_HR];
+                    sym[BS_NB0 + 7] = nb.v[Q_HPHI];
+                    for (int t = 0; t < j; ++t) sym[BS_CUR0 + t] = out.v[t];
+                }
+                val = eval_code(v.bc.code + d.code[j], v.bc.consts, sym);
+                break;
+            }
+            default: val = keep.v[j]; break;
+        }
+        out.v[j] = val;
+        if (have_sym) sym[BS_CUR0 + j] = val;
+    }
+}
+
+// Physical primitives of (1, m) after the L_LO face; covered = false if no
+// L_LO segment covers m (then the cell keeps its value).
+MPD_HD bool l_lo_out(const BcView &v, int m, Prim &out) {
+    const int s = last_cover(v, FACE_L_LO, m, v.bc.nseg[FACE_L_LO] - 1);
+    if (s < 0) return false;
+    const Prim nb = prim_of((m >= 2 && m <= v.g.M) ? central_phys(v, 2, m) : old_phys(v, 2, m));
+    eval_segment(v, v.bc.seg[v.bc.first[FACE_L_LO] + s], 1, m, 2, m, nb, nb, out);
+    return true;
+}
+
+// Primitives of (l, M+1) after the M_HI face (applied after L_LO).
+MPD_HD bool m_hi_out(const BcView &v, int l, Prim &out) {
+    const int s = last_cover(v, FACE_M_HI, l, v.bc.nseg[FACE_M_HI] - 1);
+    if (s < 0) return false;
+    const int M = v.g.M;
+    Prim nb;
+    if (l == 1) {
+        if (!l_lo_out(v, M, nb)) nb = prim_of(central_phys(v, 1, M));
+    } else {
+        nb = prim_of(central_phys(v, l, M));
+    }
+    eval_segment(v, v.bc.seg[v.bc.first[FACE_M_HI] + s], l, M + 1, l, M, nb, nb, out);
+    return true;
+}
+
+// Primitives of (l, 1), 2 <= l <= L-1, after the M_LO segments 0..limit have
+// been applied in order (each covering segment starts from the previous
+// one's result; AxisLF fields keep it).  Returns the last applied segment or -1.
+MPD_HD int m_lo_after(const BcView &v, int l, int limit, Prim &out) {
+    out = prim_of(old_phys(v, l, 1));
+    const int base = v.bc.first[FACE_M_LO];
+    int last = -1;
+    bool have_nb = false;
+    Prim nb;
+    for (int s = 0; s <= limit; ++s) {
+        const SegDesc &d = v.bc.seg[base + s];
+        if (l < d.lo || l > d.hi) continue;
+        if (!have_nb) {
+            nb = prim_of(central_phys(v, l, 2));
+            have_nb = true;
+        }
+        const Prim keep = out;
+        eval_segment(v, d, l, 1, l, 2, nb, keep, out);
+        last = s;
+    }
+    return last;
+}
+
+// Primitives of (L, m) after the L_HI face (applied last).
+MPD_HD bool l_hi_out(const BcView &v, int m, Prim &out) {
+    const int s = last_cover(v, FACE_L_HI, m, v.bc.nseg[FACE_L_HI] - 1);
+    if (s < 0) return false;
+    const int L = v.g.L, M = v.g.M;
+    Prim nb;
+    if (m >= 2 && m <= M) {
+        nb = prim_of(central_phys(v, L - 1, m));
+    } else if (m == 1) {
+        if (m_lo_after(v, L - 1, v.bc.nseg[FACE_M_LO] - 1, nb) < 0)
+            nb = prim_of(old_phys(v, L - 1, 1));
+    } else {
+        if (!m_hi_out(v, L - 1, nb)) nb = prim_of(old_phys(v, L - 1, M + 1));
+    }
+    eval_segment(v, v.bc.seg[v.bc.first[FACE_L_HI] + s], L, m, L - 1, m, nb, nb, out);
+    return true;
+}
+
+// Values AxisLF reads at the four stencil points of (l, 1).
+struct AxisPoint {
+    double u0, r, vz, vr, Hz, Hr, P, p;
+};
+
+// PerFieldBC::AxisLfU1/U2/U5/U7 (src/bcs/per_field_bc.cpp:490-566).
+// Points: C = (l,1), N = (l+1,1), S = (l-1,1), E = (l,2).
+MPD_HD double axis_u1(const AxisPoint &C, const AxisPoint &N, const AxisPoint &S,
+                      const AxisPoint &E, double dt, double dz, double dr_l) {
+    return (0.25 * (N.u0 / N.r + S.u0 / S.r + E.u0 / E.r + C.u0 / C.r)
+            + dt * (-(N.u0 / N.r * N.vz - S.u0 / S.r * S.vz) / (2.0 * dz)
+                    - (E.u0 / E.r * E.vr - C.u0 / C.r * E.vr) / dr_l))
+           * C.r;
+}
+MPD_HD double axis_u2(const AxisPoint &C, const AxisPoint &N, const AxisPoint &S,
+                      const AxisPoint &E, double dt, double dz, double dr_l) {
+    return (0.25 * (N.u0 / N.r + S.u0 / S.r + E.u0 / E.r + C.u0 / C.r)
+            + dt * (((N.Hz * N.Hz - N.P) - (S.Hz * S.Hz - S.P)) / (2.0 * dz)
+                    + (E.Hz * E.Hr - C.Hz * C.Hr) / dr_l
+                    - (N.u0 / N.r * N.vz - S.u0 / S.r * S.vz) / (2.0 * dz)
+                    - (E.u0 / E.r * E.vr - C.u0 / C.r * C.vr) / dr_l))
+           * C.r;
+}
+MPD_HD double axis_u5(const AxisPoint &C, const AxisPoint &N, const AxisPoint &S,
+                      const AxisPoint &E, double dt, double dz, double dr_l) {
+    return (0.25 * (N.u0 / N.r + S.u0 / S.r + E.u0 / E.r + C.u0 / C.r)
+            + dt * (-C.p * ((N.vz - S.vz) / (2.0 * dz) + (E.vr - C.vr) / dr_l)
+                    - (N.u0 / N.r * N.vz - S.u0 / S.r * S.vz) / (2.0 * dz)
+                    - (E.u0 / E.r * E.vr - C.u0 / C.r * C.vr) / dr_l))
+           * C.r;
+}
+MPD_HD double axis_u7(const AxisPoint &C, const AxisPoint &N, const AxisPoint &S,
+                      const AxisPoint &E, double dt, double dz, double dr_l) {
+    (void)N;
+    (void)S;
+    (void)dz;
+    return (0.25 * (N.u0 / N.r + S.u0 / S.r + E.u0 / E.r + C.u0 / C.r)
+            + dt * ((E.Hr * E.vz - C.Hr * C.vz) / dr_l
+                    - (E.u0 / E.r * E.vr - C.u0 / C.r * C.vr) / dr_l))
+           * C.r;
+}
+
+// Final conserved values of M_LO cell (l, 1): rebuild from the primitives of
+// the last covering segment, then that segment's AxisLF overwrites.  The
+// neighbours (l-1,1) / (l+1,1) are seen as the serial segment loop leaves
+// them: l-1 already processed by the same segment, l+1 not yet.
+MPD_HD void m_lo_final_u(const BcView &v, int l, int s_last, const Prim &q, double u[8]) {
+    const Geo &g = v.g;
+    Phys cur;
+    cur.rho = q.v[Q_RHO];
+    cur.vz = q.v[Q_VZ];
+    cur.vr = q.v[Q_VR];
+    cur.vphi = q.v[Q_VPHI];
+    cur.Hz = q.v[Q_HZ];
+    cur.Hr = q.v[Q_HR];
+    cur.Hphi = q.v[Q_HPHI];
+    cur.e = q.v[Q_E];
+    const double rc = g.r(l, 1);
+    rebuild_u(cur, rc, u);
+    const SegDesc &d = v.bc.seg[v.bc.first[FACE_M_LO] + s_last];
+    if (!d.has_axis) return;
+
+    // old physical state of the cell supplies p and P (never written by BCs)
+    const Phys oc = old_phys(v, l, 1);
+    // neighbour l-1
+    Prim qs;
+    if (l - 1 == 1) {
+        if (!l_lo_out(v, 1, qs)) qs = prim_of(old_phys(v, 1, 1));
+    } else {
+        const int lim = (l - 1 >= d.lo && l - 1 <= d.hi) ? s_last : s_last - 1;
+        m_lo_after(v, l - 1, lim, qs);
+    }
+    // neighbour l+1
+    Prim qn;
+    if (l + 1 == g.L) {
+        qn = prim_of(old_phys(v, g.L, 1));
+    } else {
+        m_lo_after(v, l + 1, s_last - 1, qn);
+    }
+    const Phys os = old_phys(v, l - 1, 1);
+    const Phys on = old_phys(v, l + 1, 1);
+    const Phys ce = central_phys(v, l, 2);
+
+    AxisPoint C, N, S, E;
+    C.r = rc;
+    C.vz = cur.vz;
+    C.vr = cur.vr;
+    C.Hz = cur.Hz;
+    C.Hr = cur.Hr;
+    C.P = oc.P;
+    C.p = oc.p;
+    N.r = g.r(l + 1, 1);
+    N.vz = qn.v[Q_VZ];
+    N.vr = qn.v[Q_VR];
+    N.Hz = qn.v[Q_HZ];
+    N.Hr = qn.v[Q_HR];
+    N.P = on.P;
+    N.p = on.p;
+    S.r = g.r(l - 1, 1);
+    S.vz = qs.v[Q_VZ];
+    S.vr = qs.v[Q_VR];
+    S.Hz = qs.v[Q_HZ];
+    S.Hr = qs.v[Q_HR];
+    S.P = os.P;
+    S.p = os.p;
+    E.r = g.r(l, 2);
+    E.vz = ce.vz;
+    E.vr = ce.vr;
+    E.Hz = ce.Hz;
+    E.Hr = ce.Hr;
+    E.P = ce.P;
+    E.p = ce.p;
+    const size_t ic = g.ix(l, 1), in = g.ix(l + 1, 1), is = g.ix(l - 1, 1), ie = g.ix(l, 2);
+    const double dr_l = g.dr[l];
+    // u0 planes: u_1 = k 0, u_2 = k 1, u_5 = k 4, u_7 = k 6
+    const int kcons[4] = {0, 1, 4, 6};
+    const int kprim[4] = {Q_RHO, Q_VZ, Q_E, Q_HZ};
+    for (int t = 0; t < 4; ++t) {
+        if (d.type[kprim[t]] != COND_AXIS_LF) continue;
+        const size_t off = (size_t)kcons[t] * g.ps;
+        C.u0 = v.u0[off + ic];
+        N.u0 = v.u0[off + in];
+        S.u0 = v.u0[off + is];
+        E.u0 = v.u0[off + ie];
+        double val;
+        switch (t) {
+            case 0: val = axis_u1(C, N, S, E, v.dt, g.dz, dr_l); break;
+            case 1: val = axis_u2(C, N, S, E, v.dt, g.dz, dr_l); break;
+            case 2: val = axis_u5(C, N, S, E, v.dt, g.dz, dr_l); break;
+            default: val = axis_u7(C, N, S, E, v.dt, g.dz, dr_l); break;
+        }
+        u[kcons[t]] = val;
+    }
+}
+
+MPD_HD void phys_to_prim_u(const Prim &q, double r, double u[8]) {
+    Phys p;
+    p.rho = q.v[Q_RHO];
+    p.vz = q.v[Q_VZ];
+    p.vr = q.v[Q_VR];
+    p.vphi = q.v[Q_VPHI];
+    p.Hz = q.v[Q_HZ];
+    p.Hr = q.v[Q_HR];
+    p.Hphi = q.v[Q_HPHI];
+    p.e = q.v[Q_E];
+    p.p = p.P = 0.0;
+    rebuild_u(p, r, u);
+}
+
+// Number of boundary-ring cells: rows l = 1 and l = L (m = 1..M+1) and
+// columns m = 1 and m = M+1 (l = 2..L-1).
+MPD_HD int ring_count(const Geo &g) { return 2 * (g.M + 1) + 2 * (g.L - 2); }
+
+MPD_HD void ring_cell(const Geo &g, int i, int &l, int &m) {
+    const int row = g.M + 1;
+    if (i < row) { l = 1; m = 1 + i; return; }
+    i -= row;
+    if (i < row) { l = g.L; m = 1 + i; return; }
+    i -= row;
+    if (i < g.L - 2) { l = 2 + i; m = 1; return; }
+    i -= g.L - 2;
+    l = 2 + i;
+    m = g.M + 1;
+}
+
+// Final conserved values of boundary-ring cell (l, m) after the four faces
+// L_LO, M_HI, M_LO, L_HI have been applied in that order
+// (src/solver.cpp:29-32).  The last face that covers the cell decides it;
+// cells no face covers keep the central update (interior columns) or the
+// zero the reference's never-written u arrays hold (wall columns).
+MPD_HD void bc_ring_final(const BcView &v, int l, int m, double u[8]) {
+    const Geo &g = v.g;
+    const int L = g.L, M = g.M;
+    Prim q;
+    if (l == L && l_hi_out(v, m, q)) {
+        phys_to_prim_u(q, g.r(l, m), u);
+        return;
+    }
+    if (m == 1 && l >= 2 && l <= L - 1) {
+        const int s_last = m_lo_after(v, l, v.bc.nseg[FACE_M_LO] - 1, q);
+        if (s_last >= 0) {
+            m_lo_final_u(v, l, s_last, q, u);
+            return;
+        }
+    }
+    if (m == M + 1 && m_hi_out(v, l, q)) {
+        phys_to_prim_u(q, g.r(l, m), u);
+        return;
+    }
+    if (l == 1 && l_lo_out(v, m, q)) {
+        phys_to_prim_u(q, g.r(l, m), u);
+        return;
+    }
+    if (m >= 2 && m <= M) {
+        load_cons(v.u, g.ps, g.ix(l, m), u);
+        return;
+    }
+    for (int k = 0; k < 8; ++k) u[k] = 0.0;
+}
+
+}  // namespace mpd

@@ -1,0 +1,221 @@
+"""``GpuSolver``: the drop-in for the reference's ``Solver`` on one B200.
+
+Method names follow the reference classes they replace (Solver::Advance,
+Diagnostics::ComputeDt / MaxWaveSpeed / SolutionChange / GetMassFlux /
+GetThrust, Fields::SavePrev, Verification::ComputeIntegrals /
+CheckRadialSymmetry), and ``run`` is the graph-resident form of the driver
+loop of src/main.cpp:191-282.  All state lives on the device; everything is a
+call through the C ABI of include/mpd_b200.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+
+import numpy as np
+
+from . import _native as N
+from .config import CConfig, SimConfig
+from .geometry import GeometryRegistry, Grid
+from .ic import ArrayIC, ExpressionIC, IInitialCondition
+
+PRECISIONS = {"exact": N.PRECISION_EXACT, "fast": N.PRECISION_FAST}
+
+
+@dataclasses.dataclass
+class RunResult:
+    steps: int
+    t: float
+    dt: float
+    residual: float
+    change: float
+    max_wave_speed: float
+    converged: bool
+    status: int
+    device_ms: float
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(N.DP)
+
+
+class GpuSolver:
+    """One solve on the GPU.
+
+    ``GpuSolver(cfg, grid, ic)`` does what the reference's main does between
+    the Grid and the time loop: InitPhysical (``ic``), InitConservative,
+    SavePrev when convergence checking is on, and the Solver ctor (boundary
+    configuration validated and compiled).
+    """
+
+    def __init__(self, cfg: SimConfig, grid: Grid, ic: IInitialCondition | np.ndarray,
+                 precision: str = "fast", with_prev: bool | None = None):
+        self.lib = N.load()
+        self.cfg = cfg
+        self.grid = grid
+        phys = ArrayIC(ic).Apply(grid, cfg) if isinstance(ic, np.ndarray) else ic.Apply(grid, cfg)
+        self.shape = (cfg.L_max + 2, cfg.M_max + 3)
+        if with_prev is None:
+            with_prev = cfg.convergence_threshold > 0.0
+        self.with_prev = with_prev
+        self._cc = CConfig(cfg, grid.r_0, PRECISIONS[precision], with_prev)
+        self._prof = [np.ascontiguousarray(a, dtype=np.float64) for a in grid.profiles()]
+        geo = N.Geometry(*(_dp(a) for a in self._prof))
+        phys = np.ascontiguousarray(phys, dtype=np.float64)
+        h = C.c_void_p()
+        N.check(self.lib.mpd_create(self._cc.ptr, C.byref(geo), _dp(phys), C.byref(h)), self.lib)
+        self.h = h
+        self.precision = precision
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mpd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _call(self, name, *args):
+        N.check(getattr(self.lib, name)(self.h, *args), self.lib)
+
+    # -- hot path ---------------------------------------------------------------
+    def Advance(self, dt: float) -> None:
+        """Solver::Advance (src/solver.cpp:22-37); asynchronous."""
+        self._call("mpd_advance", float(dt))
+
+    def run(self, T: float = float("inf"), dt: float | None = None, adaptive: bool | None = None,
+            max_steps: int = 1 << 40, residual_tol: float = 0.0, residual_every: int = 1,
+            convergence_threshold: float | None = None, check_frequency: int | None = None,
+            steps_per_graph: int = 0) -> RunResult:
+        """Graph-resident driver loop (src/main.cpp:191-282)."""
+        cfg = self.cfg
+        p = N.RunParams()
+        p.T = T
+        p.dt = cfg.dt if dt is None else dt
+        p.adaptive = int(cfg.adaptive_dt if adaptive is None else adaptive)
+        p.cfl_number, p.dt_growth_factor = cfg.cfl_number, cfg.dt_growth_factor
+        p.dt_min, p.dt_max = cfg.dt_min, cfg.dt_max
+        p.convergence_threshold = (cfg.convergence_threshold if convergence_threshold is None
+                                   else convergence_threshold)
+        p.check_frequency = cfg.check_frequency if check_frequency is None else check_frequency
+        p.residual_tol = residual_tol
+        p.residual_every = residual_every
+        p.max_steps = int(max_steps)
+        p.steps_per_graph = steps_per_graph
+        st = N.RunStats()
+        rc = self.lib.mpd_run(self.h, C.byref(p), C.byref(st))
+        if rc not in (N.MPD_OK, N.MPD_ERR_NONFINITE):
+            N.check(rc, self.lib)
+        return RunResult(st.steps, st.t, st.dt, st.residual, st.change, st.max_wave_speed,
+                         bool(st.converged), st.status, st.device_ms)
+
+    # -- diagnostics -------------------------------------------------------------
+    def _scalar(self, name) -> float:
+        out = C.c_double()
+        self._call(name, C.byref(out))
+        return out.value
+
+    def MaxWaveSpeed(self) -> float:
+        return self._scalar("mpd_max_wave_speed")
+
+    def ComputeDt(self, dt_current: float) -> float:
+        cfg = self.cfg
+        out = C.c_double()
+        self._call("mpd_compute_dt", cfg.cfl_number, cfg.dt_growth_factor, cfg.dt_min,
+                   cfg.dt_max, float(dt_current), C.byref(out))
+        return out.value
+
+    def SolutionChange(self) -> float:
+        return self._scalar("mpd_solution_change")
+
+    def SavePrev(self) -> None:
+        self._call("mpd_save_prev")
+
+    def CheckRadialSymmetry(self) -> float:
+        return self._scalar("mpd_radial_symmetry")
+
+    def residual(self) -> float:
+        return self._scalar("mpd_residual")
+
+    def ComputeIntegrals(self) -> np.ndarray:
+        out = np.zeros(7)
+        self._call("mpd_integrals", _dp(out))
+        return out
+
+    def outlet(self):
+        a, b = C.c_double(), C.c_double()
+        self._call("mpd_outlet", C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def GetMassFlux(self) -> float:
+        return self.outlet()[0]
+
+    def GetThrust(self) -> float:
+        return self.outlet()[1]
+
+    def probe(self, l_global: int, m_global: int) -> np.ndarray:
+        out = np.zeros(10)
+        self._call("mpd_probe", int(l_global), int(m_global), _dp(out))
+        return out
+
+    def time(self):
+        t = C.c_double()
+        s = C.c_longlong()
+        self._call("mpd_time", C.byref(t), C.byref(s))
+        return t.value, s.value
+
+    # -- state -------------------------------------------------------------------
+    def download(self, which: int) -> np.ndarray:
+        out = np.empty(self.shape)
+        self._call("mpd_download", int(which), _dp(out))
+        return out
+
+    def conserved(self) -> np.ndarray:
+        return np.stack([self.download(k) for k in range(8)])
+
+    def physical(self) -> np.ndarray:
+        return np.stack([self.download(8 + k) for k in range(10)])
+
+    def set_physical(self, phys10: np.ndarray) -> None:
+        a = np.ascontiguousarray(phys10, dtype=np.float64)
+        self._call("mpd_set_physical", _dp(a))
+
+    def stream_handle(self) -> int:
+        s = C.c_void_p()
+        self._call("mpd_get_stream", C.byref(s))
+        return s.value or 0
+
+    def profile_kernels(self, steps: int, dt: float):
+        """Mean device ms per launch of (interior kernel, boundary kernel)."""
+        out = np.zeros(2)
+        self._call("mpd_profile_kernels", int(steps), float(dt), _dp(out))
+        return float(out[0]), float(out[1])
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        self._call("mpd_device_bytes", C.byref(b))
+        return b.value
+
+
+def build_case(cfg: SimConfig, precision: str = "fast", with_prev: bool | None = None,
+               ic: IInitialCondition | None = None) -> GpuSolver:
+    """Everything src/main.cpp does before the time loop, from a SimConfig."""
+    geom = GeometryRegistry.Instance().Create(cfg.geometry.type, cfg.geometry.params)
+    grid = Grid(cfg, geom)
+    if ic is None:
+        if cfg.initial_conditions.vtk_file:
+            from .io import VtkIC
+            ic = VtkIC(cfg.initial_conditions.vtk_file)
+        else:
+            ic = ExpressionIC(cfg.initial_conditions.params)
+    return GpuSolver(cfg, grid, ic, precision=precision, with_prev=with_prev)

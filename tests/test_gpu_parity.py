@@ -1,0 +1,229 @@
+"""Parity of the CUDA path with the oracle, through the C ABI.
+
+Exact mode must reproduce the oracle (itself pinned bit for bit to the
+reference's own build) bit for bit; fast mode must stay within 1e-12
+relative L-inf per field after 1000 steps of the plain-method channel
+(200 x 80, the CPU-runnable workload).
+"""
+import numpy as np
+import pytest
+
+from oracle import bind
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+FAST_TOL = 1e-12  # relative L-inf per field after 1000 steps
+
+
+def rel_linf(a, b):
+    den = np.abs(b).max()
+    return float(np.abs(a - b).max() / (den if den > 0 else 1.0))
+
+
+def step_both(solver, oracle, cfg, n, dt):
+    """Advance both with the driver's adaptive dt; dt must agree bit for bit."""
+    for _ in range(n):
+        solver.Advance(dt)
+        oracle.advance(dt)
+        if cfg.adaptive_dt:
+            d_gpu = solver.ComputeDt(dt)
+            d_ref = oracle.compute_dt(cfg.cfl_number, cfg.dt_growth_factor, cfg.dt_min,
+                                      cfg.dt_max, dt)
+            assert d_gpu == d_ref
+            dt = d_ref
+    return dt
+
+
+@pytest.mark.parametrize("name,cfg,dt0,nsteps", [
+    ("channel_sine", cases.channel_config(L=24, M=12, a=0.1), 1e-4, 30),
+    ("reference_default", cases.reference_default_config(L=80, M=40), 1e-6, 40),
+    ("edge_segments", cases.edge_config(), 1e-4, 40),
+])
+def test_exact_bitwise_per_step(pkg, name, cfg, dt0, nsteps):
+    case = cases.make_case(cfg)
+    solver = pkg.GpuSolver(case.cfg, case.grid, case.phys, precision="exact")
+    oracle = bind.Port(case.oracle_dict())
+    dt = dt0
+    for chunk in range(4):
+        dt = step_both(solver, oracle, cfg, nsteps // 4, dt)
+        np.testing.assert_array_equal(solver.conserved(), oracle.conserved())
+    np.testing.assert_array_equal(solver.physical(), oracle.physical())
+    solver.close()
+
+
+def test_config1_exact_run_1000_steps(pkg):
+    """Plain method, 200 x 80, CFL 0.4, fixed 1000 steps: graph-resident loop."""
+    case = cases.channel_case(L=200, M=80)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="exact")
+    res = solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=1000, steps_per_graph=64)
+    oracle = bind.Port(case.oracle_dict())
+    out = oracle.run(T=1e300, dt0=cfg.dt, adaptive=True, cfl=cfg.cfl_number,
+                     growth=cfg.dt_growth_factor, dt_min=cfg.dt_min, dt_max=cfg.dt_max,
+                     max_steps=1000)
+    assert res.steps == out["steps"] == 1000
+    assert res.t == out["t"] and res.dt == out["dt"]
+    np.testing.assert_array_equal(solver.conserved(), oracle.conserved())
+    np.testing.assert_array_equal(solver.physical(), oracle.physical())
+    solver.close()
+
+
+def test_config1_fast_run_1000_steps(pkg):
+    case = cases.channel_case(L=200, M=80)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+    res = solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=1000)
+    oracle = bind.Port(case.oracle_dict())
+    out = oracle.run(T=1e300, dt0=cfg.dt, adaptive=True, cfl=cfg.cfl_number,
+                     growth=cfg.dt_growth_factor, dt_min=cfg.dt_min, dt_max=cfg.dt_max,
+                     max_steps=1000)
+    assert res.steps == 1000
+    assert abs(res.t - out["t"]) <= FAST_TOL * out["t"]
+    got, want = solver.physical(), oracle.physical()
+    for k in range(10):
+        assert rel_linf(got[k], want[k]) <= FAST_TOL, bind.PHYS_FIELDS[k]
+    got, want = solver.conserved(), oracle.conserved()
+    for k in range(8):
+        assert rel_linf(got[k], want[k]) <= FAST_TOL, f"u_{k + 1}"
+    solver.close()
+
+
+def test_fast_reference_default_and_edge(pkg):
+    for cfg, dt0 in ((cases.reference_default_config(L=80, M=40), 1e-6), (cases.edge_config(), 1e-4)):
+        case = cases.make_case(cfg)
+        solver = pkg.GpuSolver(case.cfg, case.grid, case.phys, precision="fast")
+        oracle = bind.Port(case.oracle_dict())
+        dt = dt0
+        for _ in range(200):
+            solver.Advance(dt)
+            oracle.advance(dt)
+            dt = oracle.compute_dt(cfg.cfl_number, cfg.dt_growth_factor, cfg.dt_min, cfg.dt_max, dt)
+        got, want = solver.conserved(), oracle.conserved()
+        for k in range(8):
+            assert rel_linf(got[k], want[k]) <= FAST_TOL
+        solver.close()
+
+
+def test_diagnostics_match_oracle(pkg):
+    case = cases.channel_case(L=40, M=20, a=0.12)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="exact", with_prev=True)
+    oracle = bind.Port(case.oracle_dict(with_prev=True))
+    # before any step the diagnostics read the initial condition
+    assert solver.MaxWaveSpeed() == oracle.max_wave_speed()
+    assert solver.CheckRadialSymmetry() == oracle.radial_symmetry()
+    dt = step_both(solver, oracle, cfg, 25, 1e-4)
+    assert solver.MaxWaveSpeed() == oracle.max_wave_speed()
+    assert solver.ComputeDt(dt) == oracle.compute_dt(cfg.cfl_number, cfg.dt_growth_factor,
+                                                     cfg.dt_min, cfg.dt_max, dt)
+    assert solver.CheckRadialSymmetry() == oracle.radial_symmetry()
+    mf, th = solver.outlet()
+    omf, oth = oracle.outlet()
+    assert (mf, th) == (omf, oth)          # serial trapezoid, same order
+    np.testing.assert_allclose(solver.ComputeIntegrals(), oracle.integrals(), rtol=1e-13, atol=0)
+    ch = solver.SolutionChange()
+    assert abs(ch - oracle.solution_change()) <= 1e-12 * max(ch, 1e-300)
+    solver.SavePrev()
+    oracle.save_prev()
+    step_both(solver, oracle, cfg, 5, dt)
+    ch = solver.SolutionChange()
+    assert abs(ch - oracle.solution_change()) <= 1e-12 * max(ch, 1e-300)
+    probe = solver.probe(20, 10)
+    phys = oracle.physical()
+    np.testing.assert_array_equal(probe, phys[:, 21, 11])
+    solver.close()
+
+
+def test_run_convergence_check_matches_driver(pkg):
+    """Relative-L2 convergence every check_frequency steps (src/main.cpp:233-247)."""
+    case = cases.channel_case(L=32, M=16)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="exact", with_prev=True)
+    res = solver.run(T=1e300, dt=cfg.dt, adaptive=True, convergence_threshold=5e-3,
+                     check_frequency=20, max_steps=5000, steps_per_graph=40)
+    oracle = bind.Port(case.oracle_dict(with_prev=True))
+    out = oracle.run(T=1e300, dt0=cfg.dt, adaptive=True, cfl=cfg.cfl_number,
+                     growth=cfg.dt_growth_factor, dt_min=cfg.dt_min, dt_max=cfg.dt_max,
+                     conv_threshold=5e-3, check_frequency=20, max_steps=5000)
+    assert res.converged == out["converged"]
+    assert res.steps == out["steps"]
+    assert abs(res.change - out["change"]) <= 1e-12 * out["change"]
+    np.testing.assert_array_equal(solver.conserved(), oracle.conserved())
+    solver.close()
+
+
+def test_t_clamp_and_residual(pkg):
+    """The last step is clamped to T (src/main.cpp:221-223); residual matches numpy."""
+    case = cases.channel_case(L=24, M=12)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="exact")
+    res = solver.run(T=0.05, dt=cfg.dt, adaptive=True)
+    oracle = bind.Port(case.oracle_dict())
+    out = oracle.run(T=0.05, dt0=cfg.dt, adaptive=True, cfl=cfg.cfl_number,
+                     growth=cfg.dt_growth_factor, dt_min=cfg.dt_min, dt_max=cfg.dt_max)
+    assert res.steps == out["steps"]
+    assert res.t == out["t"]
+    np.testing.assert_array_equal(solver.conserved(), oracle.conserved())
+    before = solver.conserved()
+    solver.Advance(1e-4)
+    after = solver.conserved()
+    inner = (slice(None), slice(1, -1), slice(1, -1))
+    num = np.abs(after[inner] - before[inner]).reshape(8, -1).max(axis=1)
+    den = np.maximum(np.abs(before[inner]).reshape(8, -1).max(axis=1), 1e-300)
+    assert solver.residual() == float((num / den).max())
+    solver.close()
+
+
+def test_restart_set_physical_and_snapshot(pkg):
+    case = cases.channel_case(L=24, M=12, a=0.05)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="exact")
+    solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=50)
+    phys = solver.physical()
+    # restart from the downloaded physical state == a fresh solver from it
+    other = pkg.GpuSolver(cfg, case.grid, phys, precision="exact")
+    solver.set_physical(phys)
+    for s in (solver, other):
+        s.Advance(2e-4)
+    np.testing.assert_array_equal(solver.conserved(), other.conserved())
+    # async snapshot into pinned memory equals the synchronous download
+    import torch
+    buf = torch.empty((10,) + solver.shape, dtype=torch.float64).pin_memory()
+    import ctypes
+    lib = solver.lib
+    rc = lib.mpd_snapshot_async(solver.h, ctypes.cast(ctypes.c_void_p(buf.data_ptr()),
+                                                      pkg._native.DP))
+    assert rc == 0
+    assert lib.mpd_snapshot_wait(solver.h) == 0
+    np.testing.assert_array_equal(buf.numpy(), solver.physical())
+    solver.close()
+    other.close()
+
+
+def test_config2_size_fast_vs_oracle(pkg):
+    """Full config-2 grid (1600 x 640): fast path vs the oracle over 30 steps."""
+    case = cases.channel_case(L=1600, M=640)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+    oracle = bind.Port(case.oracle_dict())
+    dt = cfg.dt
+    for _ in range(30):
+        solver.Advance(dt)
+        oracle.advance(dt)
+        dt = oracle.compute_dt(cfg.cfl_number, cfg.dt_growth_factor, cfg.dt_min, cfg.dt_max, dt)
+    got, want = solver.conserved(), oracle.conserved()
+    for k in range(8):
+        assert rel_linf(got[k], want[k]) <= FAST_TOL
+    solver.close()
+
+
+def test_bad_config_is_rejected_before_device_work(pkg):
+    cfg = cases.channel_config(L=24, M=12)
+    cfg.bc_l_lo.segments[0].rho = pkg.FieldCond("axis_lf")
+    case_geo = pkg.Grid(cfg, pkg.GeometryRegistry.Instance().Create("sine_wall", cfg.geometry.params))
+    phys = np.zeros((10, 26, 15))
+    with pytest.raises(pkg._native.MpdError) as ei:
+        pkg.GpuSolver(cfg, case_geo, phys)
+    assert ei.value.code == pkg._native.MPD_ERR_INVALID
+    assert "AxisLF condition is only valid on the M_LO face" in str(ei.value)
