@@ -194,6 +194,29 @@ int mpd_device_bytes(mpd_solver *s, size_t *bytes);
  * the interior kernel (out_ms[0]) and the boundary kernel (out_ms[1]). */
 int mpd_profile_kernels(mpd_solver *s, int steps, double dt, double out_ms[2]);
 
+/* ---- conserved integrals without allocating ----------------------------------- */
+/* No counterpart in the reference.  For callers that cannot let a library call
+ * cudaMalloc: a host whose framework owns every byte of device memory through
+ * its own pool (a stray cudaMalloc bypasses the pool's accounting, or fails
+ * once the pool has reserved the device), or one that has already handed its
+ * device memory budget out.  Computes the same 7 sums as mpd_integrals
+ * (Verification::ComputeIntegrals) over caller-owned device memory:
+ *   d_u    the 8 conserved planes, plane k at d_u + k*plane_stride, cell (l,m)
+ *          at l*pitch + m (ghost layer included, pitch >= M_max+3);
+ *   d_dr   the L_max+2 row widths dr[l] = (r_outer - r_inner)/M_max;
+ *   d_out7 receives the 7 sums (device memory).
+ * Work is enqueued on `stream` (a cudaStream_t; NULL = the default stream)
+ * and not waited for.  Its only scratch is a fixed device array of 8192 rows
+ * x 7 doubles (458,752 bytes) that every GPU loading the library keeps until
+ * the process exits; L_max > 8192 is rejected with MPD_ERR_INVALID.  The
+ * first call on a device looks up that array's device address, so make it
+ * before any stream capture.  All calls share the one array and each rewrites
+ * the rows it uses: calls whose work overlaps on the GPU race.  Calls no
+ * cudaMalloc, cudaFree or allocating library routine. */
+int mpd_integrals_noalloc(const double *d_u, size_t plane_stride, int pitch, int L_max,
+                          int M_max, const double *d_dr, double dz, double *d_out7,
+                          void *stream);
+
 /* ---- host-side expression initial condition ---------------------------------- */
 /* ExpressionIC::Apply, src/ics/expression_ic.cpp:286-324, evaluated on the host
  * with the library's expression compiler.  exprs: 8 strings in the

@@ -110,6 +110,8 @@ SIGNATURES = [
     ("mpd_get_stream", C.c_int, [_VP, C.POINTER(_VP)]),
     ("mpd_device_bytes", C.c_int, [_VP, C.POINTER(C.c_size_t)]),
     ("mpd_profile_kernels", C.c_int, [_VP, C.c_int, C.c_double, DP]),
+    ("mpd_integrals_noalloc", C.c_int, [_VP, C.c_size_t, C.c_int, C.c_int, C.c_int, _VP, C.c_double,
+                                        _VP, _VP]),
     ("mpd_expression_ic", C.c_int, [C.POINTER(Config), C.POINTER(Geometry), C.POINTER(C.c_char_p),
                                     C.c_int, C.POINTER(C.c_char_p), DP, DP]),
     ("mpd_eval_expression", C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), DP, DP]),
