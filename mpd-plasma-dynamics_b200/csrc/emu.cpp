@@ -3,7 +3,7 @@
 //
 // It runs the kernels' own per-cell functions from lf_core.cuh over every
 // cell in a plain loop: the exact interior cell (lf_exact_kernel), the fast
-// interior cell (lf_fast_kernel's fast_point / fast_cell), the boundary ring
+// interior cell (lf_tma_kernel: fast_prim / fast_a / fast_rc / fast_b / fast_finish), the boundary ring
 // (bc_kernel's bc_ring_final).  That lets the CPU suite check the boundary
 // dependency logic and the fast-mode rounding against the oracle before any
 // GPU time is spent.
@@ -32,7 +32,8 @@ struct EmuSolver {
     mpd::BcTable bc{};
     int precision = 0;
     long long step = 0;
-    double snap[16] = {};
+    int len = 0;
+    std::vector<double> cphys, wall[2];
 };
 
 }  // namespace
@@ -97,6 +98,16 @@ int mpd_emu_create(const mpd_config *cfg, const mpd_geometry *geom, const double
             mpd::rebuild_u(mpd::load_phys(s->ic.data(), ps, g.ix(l, m)), g.r(l, m), u);
             for (int k = 0; k < 8; ++k) s->buf[0][k * ps + g.ix(l, m)] = u[k];
         }
+    s->len = mpd::line_len(L, M);
+    s->cphys.assign(static_cast<size_t>(mpd::kCentralLines) * 8 * s->len, 0.0);
+    s->wall[0].assign(static_cast<size_t>(mpd::kWallLines) * 10 * s->len, 0.0);
+    s->wall[1].assign(static_cast<size_t>(mpd::kWallLines) * 10 * s->len, 0.0);
+    for (int l = 1; l <= L; ++l) {
+        mpd::store_line_phys(s->wall[0].data(), s->len, 0, l,
+                             mpd::load_phys(s->ic.data(), ps, g.ix(l, 1)));
+        mpd::store_line_phys(s->wall[0].data(), s->len, 1, l,
+                             mpd::load_phys(s->ic.data(), ps, g.ix(l, M + 1)));
+    }
     for (int f = 0; f < 4; ++f) {
         s->bc.nseg[f] = s->cbc.nseg[f];
         s->bc.first[f] = s->cbc.first[f];
@@ -104,6 +115,9 @@ int mpd_emu_create(const mpd_config *cfg, const mpd_geometry *geom, const double
     s->bc.seg = s->cbc.seg.data();
     s->bc.code = s->cbc.code.data();
     s->bc.consts = s->cbc.consts.data();
+    s->bc.nseg_total = static_cast<int>(s->cbc.seg.size());
+    s->bc.ncode = static_cast<int>(s->cbc.code.size());
+    s->bc.nconst = static_cast<int>(s->cbc.consts.size());
     s->precision = cfg->precision;
     *out = s;
     return MPD_OK;
@@ -141,18 +155,30 @@ int mpd_emu_advance(void *h, double dt, int order) {
                 }
                 mpd::lf_cell_exact(U, Q, R, dt, g.dz, g.dr[l], out);
             } else {
-                mpd::ZPoint z[5];
-                mpd::RPoint q[5];
-                for (int p = 0; p < 5; ++p) {
-                    if (ls[p] == 0 || ls[p] == g.L + 1) mpd::zero_point(z[p], q[p]);
-                    else mpd::fast_point(U[p], R[p], gm1, z[p], q[p]);
-                }
+                // the fast kernel's arithmetic, point by point (ghost rows are zero)
                 const double kz = dt * (0.5 / g.dz), kr = dt * (0.5 / g.dr[l]);
-                mpd::fast_cell(z[2], z[1], q[0], z[3].U, z[4].U, q[3].Gr, q[4].Gr, kz, kr, dt, out);
+                mpd::FastPrim q[5];
+                double Gz[5][8], Gr[5][8];
+                for (int p = 0; p < 5; ++p) {
+                    if (ls[p] == 0 || ls[p] == g.L + 1) {
+                        q[p] = mpd::FastPrim{};
+                        for (int k = 0; k < 8; ++k) Gz[p][k] = Gr[p][k] = 0.0;
+                    } else {
+                        q[p] = mpd::fast_prim(U[p], R[p], gm1);
+                        mpd::fast_gz(U[p], q[p], R[p], Gz[p]);
+                        mpd::fast_gr(U[p], q[p], R[p], Gr[p]);
+                    }
+                }
+                double A[9], B[9], ce[8], cw[8], ce_e[8], cw_w[8];
+                mpd::fast_a(U[2], Gz[2], kz, A);
+                mpd::fast_rc(U[3], Gr[3], kr, ce_e, cw);   // east neighbour's ce
+                mpd::fast_rc(U[4], Gr[4], kr, ce, cw_w);   // west neighbour's cw
+                mpd::fast_b(ce_e, cw_w, Gr[3][7], Gr[4][7], q[0], kr, dt, B);
+                mpd::fast_finish(A, B, U[1], Gz[1], kz, out);
             }
             for (int k = 0; k < 8; ++k) u[k * g.ps + g.ix(l, m)] = out[k];
-            if (m == g.M && (l == 1 || l == g.L))
-                for (int k = 0; k < 8; ++k) s->snap[(l == 1 ? 0 : 8) + k] = out[k];
+            if (mpd::wants_central(g.L, g.M, l, m))
+                mpd::store_central(s->cphys.data(), s->len, g.L, g.M, l, m, out);
         }
     }
     mpd::BcView v;
@@ -160,7 +186,9 @@ int mpd_emu_advance(void *h, double dt, int order) {
     v.u0 = u0;
     v.u = u;
     v.ic = s->ic.data();
-    v.snap = s->snap;
+    v.cphys = s->cphys.data();
+    v.wphys = s->wall[s->step & 1].data();
+    v.len = s->len;
     v.first = first ? 1 : 0;
     v.dt = dt;
     v.bc = s->bc;
@@ -172,6 +200,9 @@ int mpd_emu_advance(void *h, double dt, int order) {
         mpd::ring_cell(g, i, l, m);
         double *uf = &ring[8 * static_cast<size_t>(i)];
         mpd::bc_ring_final(v, l, m, uf);
+        if (m == 1 || m == g.M + 1)
+            mpd::store_line_phys(s->wall[(s->step + 1) & 1].data(), s->len, m == 1 ? 0 : 1, l,
+                                 mpd::recon_exact(uf, g.r(l, m), g.gamma));
         if (order != 0)
             for (int k = 0; k < 8; ++k) u[k * g.ps + g.ix(l, m)] = uf[k];
     }

@@ -23,22 +23,17 @@ struct DevState {
     double conv_thr;
     int check_freq, check_due;
     double last_ws, last_resid, last_change;
-    int ws_valid, nonfinite, resid_valid, pad1;
+    int ws_valid, nonfinite, resid_valid, wait_fail;
     unsigned long long ws_acc;
     unsigned long long num_acc[8], den_acc[8];
     unsigned int nf_acc, arrive;
-    double snap[16];
+    unsigned int res_nf, res_arrive;
+    long long resid_step;
 };
 
 constexpr int kFlagWs = 1;
-constexpr int kFlagRes = 2;
 
-__device__ __forceinline__ int step_flags(const DevState *st) {
-    int f = 0;
-    if (st->want_ws) f |= kFlagWs;
-    if (st->resid_every > 0 && ((st->step + 1) % st->resid_every) == 0) f |= kFlagRes;
-    return f;
-}
+__device__ __forceinline__ int step_flags(const DevState *st) { return st->want_ws ? kFlagWs : 0; }
 
 // Non-negative double as an order-preserving 64-bit key; NaN reported as 0
 // and flagged.
@@ -92,13 +87,12 @@ __device__ __forceinline__ void block_max_atomic(unsigned long long (&key)[NV], 
     }
 }
 
-// Accumulate the wave speed and residual contributions of a finished cell.
+// Running maximum wave speed of the cells a thread finished.
 struct CellStats {
-    unsigned long long key[17];  // 0: wave speed, 1..8: |du|, 9..16: |u0|
+    unsigned long long key[1];
     unsigned int nf;
     __device__ __forceinline__ void init() {
-#pragma unroll
-        for (int k = 0; k < 17; ++k) key[k] = 0ull;
+        key[0] = 0ull;
         nf = 0u;
     }
     __device__ __forceinline__ void add_ws(double s) {
@@ -106,24 +100,9 @@ struct CellStats {
         const unsigned long long k = max_key(s, nf);
         key[0] = k > key[0] ? k : key[0];
     }
-    __device__ __forceinline__ void add_res(const double *un, const double *uo) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const unsigned long long a = max_key(fabs(un[k] - uo[k]), nf);
-            const unsigned long long b = max_key(fabs(uo[k]), nf);
-            key[1 + k] = a > key[1 + k] ? a : key[1 + k];
-            key[9 + k] = b > key[9 + k] ? b : key[9 + k];
-        }
-    }
-    __device__ __forceinline__ void flush(DevState *st, int flags) {
-        unsigned long long *dst[17];
-        dst[0] = (flags & kFlagWs) ? &st->ws_acc : nullptr;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            dst[1 + k] = (flags & kFlagRes) ? &st->num_acc[k] : nullptr;
-            dst[9 + k] = (flags & kFlagRes) ? &st->den_acc[k] : nullptr;
-        }
-        block_max_atomic<17>(key, nf, dst, &st->nf_acc);
+    __device__ __forceinline__ void flush(DevState *st) {
+        unsigned long long *dst[1] = {&st->ws_acc};
+        block_max_atomic<1>(key, nf, dst, &st->nf_acc);
     }
 };
 
@@ -134,7 +113,8 @@ struct CellStats {
 template <bool FIRST>
 __global__ void __launch_bounds__(256) lf_exact_kernel(Geo g, double *buf0, double *buf1,
                                                        const double *__restrict__ ic, DevState *st,
-                                                       double dt_arg, int use_state_dt) {
+                                                       double dt_arg, int use_state_dt,
+                                                       double *cphys, int len) {
     if (st->done) return;
     const long long step = st->step;
     const double *__restrict__ u0 = (step & 1) ? buf1 : buf0;
@@ -165,38 +145,58 @@ __global__ void __launch_bounds__(256) lf_exact_kernel(Geo g, double *buf0, doub
         const size_t ic0 = g.ix(l, m);
 #pragma unroll
         for (int k = 0; k < 8; ++k) u[(size_t)k * g.ps + ic0] = out[k];
-        if (m == g.M && (l == 1 || l == g.L)) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) st->snap[(l == 1 ? 0 : 8) + k] = out[k];
-        }
-        if (l >= 2 && l <= g.L - 1) {  // cells no boundary face can overwrite
-            if (flags & kFlagWs) cs.add_ws(wave_speed(recon_exact(out, R[0], g.gamma), g.gamma));
-            if (flags & kFlagRes) cs.add_res(out, U[0]);
-        }
+        // cells no boundary face can overwrite feed the wave speed; cells the
+        // faces read go to the central lines
+        if ((flags & kFlagWs) && l >= 2 && l <= g.L - 1)
+            cs.add_ws(wave_speed(recon_exact(out, R[0], g.gamma), g.gamma));
+        if (wants_central(g.L, g.M, l, m)) store_central(cphys, len, g.L, g.M, l, m, out);
     }
-    if (flags) cs.flush(st, flags);
+    if (flags) cs.flush(st);
 }
 
 // Boundary faces, one thread per boundary-ring cell, plus the end-of-step
 // controller in the last block to finish.
-__global__ void __launch_bounds__(128) bc_kernel(Geo g, double *buf0, double *buf1,
+__global__ void __launch_bounds__(64) bc_kernel(Geo g, double *buf0, double *buf1,
                                                  const double *__restrict__ ic, BcTable bc,
-                                                 DevState *st, double dt_arg, int use_state_dt) {
+                                                 DevState *st, double dt_arg, int use_state_dt,
+                                                 const double *cphys, double *wall0, double *wall1,
+                                                 int len) {
     if (st->done) return;
     const long long step = st->step;
     const double *u0 = (step & 1) ? buf1 : buf0;
     double *u = (step & 1) ? buf0 : buf1;
     const double dt = use_state_dt ? st->dt : dt_arg;
     const int flags = step_flags(st);
+    // the boundary table is read many times per thread: stage it in shared memory
+    __shared__ SegDesc s_seg[kMaxSegments];
+    __shared__ int32_t s_code[kSmemCode];
+    __shared__ double s_const[kSmemConst];
+    {
+        const int nwords = bc.nseg_total * (int)(sizeof(SegDesc) / sizeof(int));
+        const int *src = reinterpret_cast<const int *>(bc.seg);
+        int *dst = reinterpret_cast<int *>(s_seg);
+        for (int w = threadIdx.x; w < nwords; w += blockDim.x) dst[w] = src[w];
+        if (bc.ncode <= kSmemCode)
+            for (int w = threadIdx.x; w < bc.ncode; w += blockDim.x) s_code[w] = bc.code[w];
+        if (bc.nconst <= kSmemConst)
+            for (int w = threadIdx.x; w < bc.nconst; w += blockDim.x) s_const[w] = bc.consts[w];
+        __syncthreads();
+    }
     BcView v;
     v.g = g;
     v.u0 = u0;
     v.u = u;
     v.ic = ic;
-    v.snap = st->snap;
+    v.cphys = cphys;
+    v.wphys = (step & 1) ? wall1 : wall0;
+    v.len = len;
     v.first = step == 0;
     v.dt = dt;
     v.bc = bc;
+    v.bc.seg = s_seg;
+    if (bc.ncode <= kSmemCode) v.bc.code = s_code;
+    if (bc.nconst <= kSmemConst) v.bc.consts = s_const;
+    double *wnext = (step & 1) ? wall0 : wall1;
     CellStats cs;
     cs.init();
     const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -208,14 +208,16 @@ __global__ void __launch_bounds__(128) bc_kernel(Geo g, double *buf0, double *bu
         const size_t ix = g.ix(l, m);
 #pragma unroll
         for (int k = 0; k < 8; ++k) u[(size_t)k * g.ps + ix] = uf[k];
-        if (flags & kFlagWs) cs.add_ws(wave_speed(recon_exact(uf, g.r(l, m), g.gamma), g.gamma));
-        if (flags & kFlagRes) {
-            double uo[8];
-            load_cons(u0, g.ps, ix, uo);
-            cs.add_res(uf, uo);
+        const bool wall = m == 1 || m == g.M + 1;
+        if ((flags & kFlagWs) || wall) {
+            // the full reconstruction of this cell: wave speed, and for the
+            // wall columns the "old" value the next step's faces read
+            const Phys q = recon_exact(uf, g.r(l, m), g.gamma);
+            if (flags & kFlagWs) cs.add_ws(wave_speed(q, g.gamma));
+            if (wall) store_line_phys(wnext, len, m == 1 ? 0 : 1, l, q);
         }
     }
-    cs.flush(st, flags);
+    if (flags) cs.flush(st);
 
     // ---- last block: finalise the step -------------------------------------
     __shared__ int is_last;
@@ -225,55 +227,123 @@ __global__ void __launch_bounds__(128) bc_kernel(Geo g, double *buf0, double *bu
     __syncthreads();
     if (!is_last || threadIdx.x != 0) return;
     __threadfence();
-    volatile DevState *vs = st;
-    double ws = 0.0;
-    if (flags & kFlagWs) {
-        ws = __longlong_as_double((long long)vs->ws_acc);
-        vs->last_ws = ws;
-        vs->ws_valid = 1;
-    } else {
-        vs->ws_valid = 0;
-    }
-    double R = 0.0;
-    if (flags & kFlagRes) {
-        for (int k = 0; k < 8; ++k) {
-            const double num = __longlong_as_double((long long)vs->num_acc[k]);
-            const double den = __longlong_as_double((long long)vs->den_acc[k]);
-            const double q = num / (den > 1e-300 ? den : 1e-300);
-            R = q > R ? q : R;
-        }
-        vs->last_resid = R;
-        vs->resid_valid = 1;
-    }
-    if (vs->nf_acc || !isfinite(R) || !isfinite(ws)) vs->nonfinite = 1;
-    const double t = vs->t + dt;
+    // All reads first, through L2 and independent of each other, so the
+    // controller costs one memory round trip instead of one per field.
+    const unsigned long long ws_bits = __ldcg(&st->ws_acc);
+    const unsigned int nf_acc = __ldcg(&st->nf_acc);
+    const double t0 = __ldcg(&st->t);
+    const int nonfinite0 = __ldcg(&st->nonfinite);
+    const int run_mode = __ldcg(&st->run_mode);
+    const int adaptive = __ldcg(&st->adaptive);
+    const double cfl = __ldcg(&st->cfl), growth = __ldcg(&st->growth);
+    const double dt_min = __ldcg(&st->dt_min), dt_max = __ldcg(&st->dt_max);
+    const double T = __ldcg(&st->T);
+    const long long max_steps = __ldcg(&st->max_steps);
+    const double conv_thr = __ldcg(&st->conv_thr);
+    const int check_freq = __ldcg(&st->check_freq);
+
+    const double ws = (flags & kFlagWs) ? __longlong_as_double((long long)ws_bits) : 0.0;
+    if (flags & kFlagWs) st->last_ws = ws;
+    st->ws_valid = (flags & kFlagWs) ? 1 : 0;
+    const int nonfinite = (nonfinite0 || nf_acc || !isfinite(ws)) ? 1 : 0;
+    st->nonfinite = nonfinite;
+    const double t = t0 + dt;
     const long long nstep = step + 1;
-    vs->t = t;
-    vs->dt_used = dt;
-    vs->step = nstep;
-    if (vs->run_mode) {
+    st->t = t;
+    st->dt_used = dt;
+    st->step = nstep;
+    st->resid_valid = 0;  // the residual of this step is evaluated on request
+    if (run_mode) {
         double dtn = dt;
-        if (vs->adaptive)
-            dtn = compute_dt_from_speed(ws, g.dz, g.dy, vs->cfl, vs->growth, vs->dt_min, vs->dt_max, dt);
-        int done = 0;
-        if ((flags & kFlagRes) && vs->resid_tol > 0.0 && R <= vs->resid_tol) {
-            vs->converged = 1;
-            done = 1;
-        }
-        if (vs->nonfinite || !(t < vs->T) || nstep >= vs->max_steps) done = 1;
-        if (t + dtn > vs->T) dtn = vs->T - t;
-        vs->dt = dtn;
-        vs->check_due = (vs->conv_thr > 0.0 && vs->check_freq > 0 && nstep % vs->check_freq == 0);
-        vs->done = done;
+        if (adaptive) dtn = compute_dt_from_speed(ws, g.dz, g.dy, cfl, growth, dt_min, dt_max, dt);
+        const int done = (nonfinite || !(t < T) || nstep >= max_steps) ? 1 : 0;
+        if (t + dtn > T) dtn = T - t;
+        st->dt = dtn;
+        st->check_due = (conv_thr > 0.0 && check_freq > 0 && nstep % check_freq == 0) ? 1 : 0;
+        st->done = done;
     }
-    vs->ws_acc = 0ull;
-    for (int k = 0; k < 8; ++k) {
-        vs->num_acc[k] = 0ull;
-        vs->den_acc[k] = 0ull;
-    }
-    vs->nf_acc = 0u;
+    st->ws_acc = 0ull;
+    st->nf_acc = 0u;
     __threadfence();
-    vs->arrive = 0u;
+    st->arrive = 0u;
+}
+
+// L-inf residual of the step that just finished (new; the reference has only
+// the relative-L2 change): R = max_k |u_k^{n+1} - u_k^n|_inf / max(|u_k^n|_inf,
+// 1e-300) over the interior cells, reading both ping-pong buffers.  In run
+// mode it also stops the loop once R <= residual_tol.  Skips a state it
+// already evaluated (a run may have stopped before this graph node).
+__global__ void __launch_bounds__(256) residual_kernel(Geo g, const double *buf0,
+                                                       const double *buf1, DevState *st) {
+    const long long step = st->step;
+    if (step == 0 || st->resid_step == step) return;
+    const double *un = (step & 1) ? buf1 : buf0;
+    const double *uo = (step & 1) ? buf0 : buf1;
+    unsigned long long key[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) key[k] = 0ull;
+    unsigned int nf = 0u;
+    const int W = g.M + 1;
+    const int total = g.L * W;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
+        const size_t i = g.ix(1 + c / W, 1 + c % W);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const double a = un[(size_t)k * g.ps + i], b = uo[(size_t)k * g.ps + i];
+            const unsigned long long d = max_key(fabs(a - b), nf);
+            const unsigned long long o = max_key(fabs(b), nf);
+            key[k] = d > key[k] ? d : key[k];
+            key[8 + k] = o > key[8 + k] ? o : key[8 + k];
+        }
+    }
+    unsigned long long *dst[16];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        dst[k] = &st->num_acc[k];
+        dst[8 + k] = &st->den_acc[k];
+    }
+    block_max_atomic<16>(key, nf, dst, &st->res_nf);
+
+    __shared__ int is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(&st->res_arrive, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!is_last || threadIdx.x != 0) return;
+    __threadfence();
+    unsigned long long num[8], den[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        num[k] = __ldcg(&st->num_acc[k]);
+        den[k] = __ldcg(&st->den_acc[k]);
+    }
+    const unsigned int res_nf = __ldcg(&st->res_nf);
+    const int run_mode = __ldcg(&st->run_mode);
+    const double resid_tol = __ldcg(&st->resid_tol);
+    const int nonfinite0 = __ldcg(&st->nonfinite);
+    double R = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const double n = __longlong_as_double((long long)num[k]);
+        const double d = __longlong_as_double((long long)den[k]);
+        const double q = n / (d > 1e-300 ? d : 1e-300);
+        R = q > R ? q : R;
+        st->num_acc[k] = 0ull;
+        st->den_acc[k] = 0ull;
+    }
+    const int nonfinite = (nonfinite0 || res_nf || !isfinite(R)) ? 1 : 0;
+    st->nonfinite = nonfinite;
+    st->res_nf = 0u;
+    st->last_resid = R;
+    st->resid_valid = 1;
+    st->resid_step = step;
+    if (run_mode && resid_tol > 0.0 && R <= resid_tol) {
+        st->converged = 1;
+        st->done = 1;
+    }
+    if (run_mode && nonfinite) st->done = 1;
+    __threadfence();
+    st->res_arrive = 0u;
 }
 
 // ---------------------------------------------------------------------------
@@ -512,6 +582,15 @@ __global__ void phys_planes_kernel(StateBufs sb, double *out) {
         out[7 * g.ps + o] = q.Hz;
         out[8 * g.ps + o] = q.Hr;
         out[9 * g.ps + o] = q.Hphi;
+    }
+}
+
+// Wall lines of step 0: the initial condition on columns 1 and M+1.
+__global__ void init_wall_kernel(Geo g, const double *ic, double *wall0, int len) {
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < g.L + 2; l += gridDim.x * blockDim.x) {
+        const bool in = l >= 1 && l <= g.L;
+        store_line_phys(wall0, len, 0, l, in ? load_phys(ic, g.ps, g.ix(l, 1)) : phys_zero());
+        store_line_phys(wall0, len, 1, l, in ? load_phys(ic, g.ps, g.ix(l, g.M + 1)) : phys_zero());
     }
 }
 

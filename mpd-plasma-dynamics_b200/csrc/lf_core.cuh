@@ -217,95 +217,153 @@ MPD_HD void lf_cell_exact(const double U[5][8], const Phys Q[5], const double R[
 }
 
 // ---------------------------------------------------------------------------
-// Fast-mode point and cell arithmetic (MPD_PRECISION_FAST, lf_fast.cuh).
+// Fast-mode arithmetic (MPD_PRECISION_FAST, lf_fast.cuh).
+//
+// Same update as lf_cell_exact, reorganised so that every stencil point is
+// evaluated once and its contributions are folded into running sums:
+//   out_k(l) = A_k(l) + B_k(l) + 0.25 U_k(l+1) + kz Gz_k(l+1)
+// with  A_k(l) = 0.25 U_k(l-1) - kz Gz_k(l-1)          (z neighbour below)
+//       B_k(l) = (U_k(m+1)/4 + kr Gr_k(m+1)) + (U_k(m-1)/4 - kr Gr_k(m-1))
+//                + dt S_k(l)                           (r neighbours, sources)
+// kz = dt / (2 dz), kr = dt / (2 dr_l); Gz / Gr are each equation's z / r
+// flux combination at a point (index 6 of Gz, free because u_7 has no z flux,
+// carries v_z r; index 7 of Gr, free because u_8 has no r flux, carries v_r r;
+// both feed u_5's -p div(r v) source).  Divides become reciprocals computed by
+// Newton iteration from a single-precision seed.
 // ---------------------------------------------------------------------------
-// Z-direction point quantities: conserved values and the z flux combination
-// of each equation (index 6, free because u_7 has no z flux, carries v_z r
-// for the -p div(r v) source of u_5).
-struct ZPoint {
-    double U[8];
-    double Gz[8];
-};
-// R-direction point quantities (index 7, free because u_8 has no r flux,
-// carries v_r r) and the cell-centred sources.
-struct RPoint {
-    double Gr[8];
-    double S3, S4, p;
-};
 
-MPD_HD void fast_point(const double U[8], double r, double gm1, ZPoint &z,
-                                           RPoint &q) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) z.U[k] = U[k];
-    const double ir = 1.0 / r;
-    const double iu = 1.0 / U[0];
-    const double rho = U[0] * ir;
-    const double vz = U[1] * iu, vr = U[2] * iu, vphi = U[3] * iu, e = U[4] * iu;
-    const double Hphi = U[5], Hz = U[6] * ir, Hr = U[7] * ir;
-    const double p = gm1 * rho * e;
-    const double P = fma(0.5, fma(Hz, Hz, fma(Hr, Hr, Hphi * Hphi)), p);
-    const double HzHr_r = Hz * Hr * r;
-    z.Gz[0] = -U[0] * vz;
-    z.Gz[1] = fma(fma(Hz, Hz, -P), r, -U[1] * vz);
-    z.Gz[2] = fma(-U[2], vz, HzHr_r);
-    z.Gz[3] = fma(Hphi * Hz, r, -U[3] * vz);
-    z.Gz[4] = -U[4] * vz;
-    z.Gz[5] = fma(Hz, vphi, -U[5] * vz);
-    z.Gz[6] = vz * r;
-    z.Gz[7] = fma(Hz * vr, r, -U[7] * vz);
-    q.Gr[0] = -U[0] * vr;
-    q.Gr[1] = fma(-U[1], vr, HzHr_r);
-    q.Gr[2] = fma(fma(Hr, Hr, -P), r, -U[2] * vr);
-    q.Gr[3] = fma(Hphi * Hr, r, -U[3] * vr);
-    q.Gr[4] = -U[4] * vr;
-    q.Gr[5] = fma(Hr, vphi, -U[5] * vr);
-    q.Gr[6] = fma(Hr * vz, r, -U[6] * vr);
-    q.Gr[7] = vr * r;
-    q.S3 = fma(rho * vphi, vphi, P) - Hphi * Hphi;
-    q.S4 = fma(-rho * vr, vphi, Hphi * Hr);
-    q.p = p;
+// 1/x for |x| in the normal single-precision range: single-precision seed
+// (relative error < 2^-22), two Newton-Raphson steps y <- y + y (1 - x y),
+// each doubling the correct bits (2^-44, then below double rounding).
+MPD_HD double rcp_nr(double x) {
+#ifdef __CUDA_ARCH__
+    float yf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"((float)x));
+    double y = (double)yf;
+#else
+    double y = (double)(1.0f / (float)x);
+#endif
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
 }
 
-MPD_HD void zero_point(ZPoint &z, RPoint &q) {
+// sqrt(a) for a in the normal single-precision range (0 -> 0, a < 0 -> NaN):
+// single-precision 1/sqrt seed, two Newton steps y <- y (3 - a y^2) / 2, then
+// s = a y with one Heron correction s <- s + y (a - s^2) / 2.
+MPD_HD double sqrt_nr(double a) {
+#ifdef __CUDA_ARCH__
+    float yf;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"((float)a));
+    double y = (double)yf;
+#else
+    double y = (double)(1.0f / sqrtf((float)a));
+#endif
+    const double ha = 0.5 * a;
+    y = y * fma(-ha * y, y, 1.5);
+    y = y * fma(-ha * y, y, 1.5);
+    const double s = a * y;
+    const double r = fma(-s, s, a);
+    const double out = fma(0.5 * y, r, s);
+    return a > 0.0 ? out : (a == 0.0 ? 0.0 : NAN);
+}
+
+// Primitive values of one point (Fields::UpdatePhysicalFromU with reciprocals).
+struct FastPrim {
+    double rho, vz, vr, vphi, e, Hphi, Hz, Hr, p, P;
+};
+
+MPD_HD FastPrim fast_prim(const double U[8], double r, double gm1) {
+    FastPrim q;
+    const double ir = rcp_nr(r);
+    const double iu = rcp_nr(U[0]);
+    q.rho = U[0] * ir;
+    q.vz = U[1] * iu;
+    q.vr = U[2] * iu;
+    q.vphi = U[3] * iu;
+    q.e = U[4] * iu;
+    q.Hphi = U[5];
+    q.Hz = U[6] * ir;
+    q.Hr = U[7] * ir;
+    q.p = gm1 * q.rho * q.e;
+    q.P = fma(0.5, fma(q.Hz, q.Hz, fma(q.Hr, q.Hr, q.Hphi * q.Hphi)), q.p);
+    return q;
+}
+
+// z flux combination of each equation at a point (Gz[6] = v_z r).
+MPD_HD void fast_gz(const double U[8], const FastPrim &q, double r, double Gz[8]) {
+    Gz[0] = -U[0] * q.vz;
+    Gz[1] = fma(fma(q.Hz, q.Hz, -q.P), r, -U[1] * q.vz);
+    Gz[2] = fma(q.Hz * q.Hr, r, -U[2] * q.vz);
+    Gz[3] = fma(q.Hphi * q.Hz, r, -U[3] * q.vz);
+    Gz[4] = -U[4] * q.vz;
+    Gz[5] = fma(q.Hz, q.vphi, -U[5] * q.vz);
+    Gz[6] = q.vz * r;
+    Gz[7] = fma(q.Hz * q.vr, r, -U[7] * q.vz);
+}
+
+// r flux combination of each equation at a point (Gr[7] = v_r r).
+MPD_HD void fast_gr(const double U[8], const FastPrim &q, double r, double Gr[8]) {
+    Gr[0] = -U[0] * q.vr;
+    Gr[1] = fma(q.Hz * q.Hr, r, -U[1] * q.vr);
+    Gr[2] = fma(fma(q.Hr, q.Hr, -q.P), r, -U[2] * q.vr);
+    Gr[3] = fma(q.Hphi * q.Hr, r, -U[3] * q.vr);
+    Gr[4] = -U[4] * q.vr;
+    Gr[5] = fma(q.Hr, q.vphi, -U[5] * q.vr);
+    Gr[6] = fma(q.Hr * q.vz, r, -U[6] * q.vr);
+    Gr[7] = q.vr * r;
+}
+
+// A(l+1) from point row l: A[k] = U/4 - kz Gz (u_7: U/4); A[8] = v_z r.
+MPD_HD void fast_a(const double U[8], const double Gz[8], double kz, double A[9]) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) A[k] = (k == 6) ? 0.25 * U[6] : fma(-kz, Gz[k], 0.25 * U[k]);
+    A[8] = Gz[6];
+}
+
+// A point's shares of its r neighbours' B: ce (seen from the cell to its west,
+// as that cell's east neighbour) = U/4 + kr Gr and cw (seen from the cell to
+// its east) = U/4 - kr Gr; for u_8, U/4 alone (its r term is u_5's source).
+MPD_HD void fast_rc(const double U[8], const double Gr[8], double kr, double ce[8],
+                    double cw[8]) {
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        const double q = 0.25 * U[k];
+        ce[k] = fma(kr, Gr[k], q);
+        cw[k] = fma(-kr, Gr[k], q);
+    }
+    ce[7] = cw[7] = 0.25 * U[7];
+}
+
+// B(l) from the east neighbour's ce, the west neighbour's cw, their v_r r
+// (g7e, g7w) and the point's own sources; B[8] = p.
+MPD_HD void fast_b(const double ce_e[8], const double cw_w[8], double g7e, double g7w,
+                   const FastPrim &q, double kr, double dt, double B[9]) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) B[k] = ce_e[k] + cw_w[k];
+    B[2] = fma(dt, fma(q.rho * q.vphi, q.vphi, q.P) - q.Hphi * q.Hphi, B[2]);
+    B[3] = fma(dt, fma(-q.rho * q.vr, q.vphi, q.Hphi * q.Hr), B[3]);
+    // r part of u_5's source -p kr (v_r r)_e - (v_r r)_w
+    B[4] = fma(-q.p * kr, g7e - g7w, B[4]);
+    B[8] = q.p;
+}
+
+// Close cell row l with point row l+1 (U, Gz).
+MPD_HD void fast_finish(const double A[9], const double B[9], const double Un[8],
+                        const double Gzn[8], double kz, double out[8]) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        z.U[k] = 0.0;
-        z.Gz[k] = 0.0;
-        q.Gr[k] = 0.0;
+        const double s = A[k] + B[k];
+        out[k] = (k == 6) ? fma(0.25, Un[6], s) : fma(kz, Gzn[k], fma(0.25, Un[k], s));
     }
-    q.S3 = q.S4 = q.p = 0.0;
+    // z part of u_5's source: -p kz ((v_z r)_n - (v_z r)_s)
+    out[4] = fma(-B[8] * kz, Gzn[6] - A[8], out[4]);
 }
 
-// One cell of the fast update from its stencil's point quantities: S/N are
-// the z neighbours, C the cell itself, E/W the r neighbours' U and Gr.
-// kz = dt/(2 dz), kr = dt/(2 dr_l).
-MPD_HD void fast_cell(const ZPoint &zS, const ZPoint &zN, const RPoint &qC, const double Ue[8],
-                      const double Uw[8], const double Ge[8], const double Gw[8], double kz,
-                      double kr, double dt, double out[8]) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const double avg = 0.25 * ((zN.U[k] + zS.U[k]) + (Ue[k] + Uw[k]));
-        double v;
-        if (k == 6) {
-            v = fma(kr, Ge[6] - Gw[6], avg);               // u_7: r flux only
-        } else if (k == 7) {
-            v = fma(kz, zN.Gz[7] - zS.Gz[7], avg);         // u_8: z flux only
-        } else {
-            v = fma(kz, zN.Gz[k] - zS.Gz[k], fma(kr, Ge[k] - Gw[k], avg));
-            if (k == 2) v = fma(dt, qC.S3, v);
-            if (k == 3) v = fma(dt, qC.S4, v);
-        }
-        out[k] = v;
-    }
-    // u_5 source -p div(r v): index 6 of Gz carries v_z r, index 7 of Gr v_r r
-    const double div = fma(kz, zN.Gz[6] - zS.Gz[6], kr * (Ge[7] - Gw[7]));
-    out[4] = fma(-qC.p, div, out[4]);
-}
-
-// Wave speed of a new cell state in the fast kernel (reciprocals instead of
-// divides, IEEE sqrt).
+// Wave speed |v| + c_s + c_a of a new cell state (reciprocals, Newton sqrt).
 MPD_HD double fast_wave_speed(const double u[8], double r, double gamma) {
-    const double ir = 1.0 / r, iu = 1.0 / u[0];
+    const double ir = rcp_nr(r), iu = rcp_nr(u[0]);
     const double rho = u[0] * ir, vz = u[1] * iu, vr = u[2] * iu;
     const double e = u[4] * iu, Hphi = u[5], Hz = u[6] * ir, Hr = u[7] * ir;
     const double prs = (gamma - 1.0) * rho * e;
@@ -313,7 +371,7 @@ MPD_HD double fast_wave_speed(const double u[8], double r, double gamma) {
     const double cs2 = gamma * prs * irho;
     const double ca2 = fma(Hz, Hz, fma(Hr, Hr, Hphi * Hphi)) * irho;
     const double v2 = fma(vz, vz, vr * vr);
-    return sqrt(v2) + sqrt(cs2) + sqrt(ca2);
+    return sqrt_nr(v2) + sqrt_nr(cs2) + sqrt_nr(ca2);
 }
 
 // ---------------------------------------------------------------------------
@@ -404,16 +462,98 @@ struct BcTable {
     const SegDesc *seg;
     const int32_t *code;
     const double *consts;
+    int nseg_total, ncode, nconst;
 };
+
+// Largest expression code / constant pools the boundary kernel stages in
+// shared memory (larger tables are read from global memory).
+constexpr int kSmemCode = 1024;
+constexpr int kSmemConst = 256;
+
+// Everything one boundary step reads.
+// Physical values of the cells the boundary faces read, laid out as "lines"
+// of 10 fields (Phys order) along one grid row or column: line stride
+// 10 * len, field stride len.
+//   central lines (the interior kernel's new conserved values, 8 fields, of
+//   the cells the faces read; the boundary kernel reconstructs them):
+//   0 = row 2 by m, 1 = row L-1 by m, 2 = column 2 by l, 3 = column M by l
+//   (its entries l = 1 and l = L are (1,M) and (L,M) before the L faces
+//   overwrite them);
+//   wall lines (the previous step's full reconstruction of the wall columns,
+//   written by the boundary kernel; the initial condition on step 0):
+//   0 = column 1 by l, 1 = column M+1 by l.
+constexpr int kCentralLines = 4;
+constexpr int kWallLines = 2;
+
+MPD_HD int line_len(int L, int M) { return (L + 2 > M + 3) ? L + 2 : M + 3; }
+
+MPD_HD Phys line_phys(const double *lines, int len, int line, int idx) {
+    const double *b = lines + (size_t)line * 10 * len + idx;
+    Phys q;
+    q.rho = b[0 * len];
+    q.vz = b[1 * len];
+    q.vr = b[2 * len];
+    q.vphi = b[3 * len];
+    q.e = b[4 * len];
+    q.p = b[5 * len];
+    q.P = b[6 * len];
+    q.Hz = b[7 * len];
+    q.Hr = b[8 * len];
+    q.Hphi = b[9 * len];
+    return q;
+}
+
+MPD_HD void store_line_phys(double *lines, int len, int line, int idx, const Phys &q) {
+    double *b = lines + (size_t)line * 10 * len + idx;
+    b[0 * len] = q.rho;
+    b[1 * len] = q.vz;
+    b[2 * len] = q.vr;
+    b[3 * len] = q.vphi;
+    b[4 * len] = q.e;
+    b[5 * len] = q.p;
+    b[6 * len] = q.P;
+    b[7 * len] = q.Hz;
+    b[8 * len] = q.Hr;
+    b[9 * len] = q.Hphi;
+}
+
+// Which central line (and index) holds cell (l, m), or -1.
+MPD_HD int central_line(int L, int M, int l, int m, int &idx) {
+    if (l == 2) { idx = m; return 0; }
+    if (l == L - 1) { idx = m; return 1; }
+    if (m == 2) { idx = l; return 2; }
+    if (m == M) { idx = l; return 3; }
+    idx = 0;
+    return -1;
+}
+
+// Store the new conserved values of a freshly updated central cell into every
+// central line that holds it (line stride 8 * len, field stride len).
+MPD_HD void store_central(double *cl, int len, int L, int M, int l, int m, const double u[8]) {
+    const int lines[4] = {l == 2 ? 0 : -1, l == L - 1 ? 1 : -1, m == 2 ? 2 : -1, m == M ? 3 : -1};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        if (lines[t] < 0) continue;
+        double *b = cl + (size_t)lines[t] * 8 * len + (t < 2 ? m : l);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) b[(size_t)k * len] = u[k];
+    }
+}
+
+MPD_HD bool wants_central(int L, int M, int l, int m) {
+    return l == 2 || l == L - 1 || m == 2 || m == M;
+}
 
 // Everything one boundary step reads.
 struct BcView {
     Geo g;
-    const double *u0;    // conserved state at the start of the step
-    double *u;           // new state (interior written by the LF kernel)
-    const double *ic;    // initial physical planes (first step only)
-    const double *snap;  // central u of (1,M) [0..7] and (L,M) [8..15] before BCs
-    int first;           // step 0: "old" physical values are the IC planes
+    const double *u0;     // conserved state at the start of the step
+    double *u;            // new state (interior written by the LF kernel)
+    const double *ic;     // initial physical planes (first step only)
+    const double *cphys;  // central lines of this step (conserved values)
+    const double *wphys;  // wall lines at the start of this step
+    int len;              // line length
+    int first;            // step 0: "old" physical values are the IC planes
     double dt;
     BcTable bc;
 };
@@ -438,7 +578,10 @@ MPD_HD Prim prim_of(const Phys &q) {
 
 // Physical value of a cell as the previous step's full reconstruction left
 // it (or the initial condition on the first step).
+// The boundary faces only ever ask for wall cells (m = 1 or M+1) here.
 MPD_HD Phys old_phys(const BcView &v, int l, int m) {
+    if (m == 1) return line_phys(v.wphys, v.len, 0, l);
+    if (m == v.g.M + 1) return line_phys(v.wphys, v.len, 1, l);
     const size_t i = v.g.ix(l, m);
     if (v.first) return load_phys(v.ic, v.g.ps, i);
     double u[8];
@@ -447,16 +590,19 @@ MPD_HD Phys old_phys(const BcView &v, int l, int m) {
 }
 
 // Physical value of a central cell after this step's central update
-// (UpdateCentralPhysical, src/solver.cpp:155-159).
+// (UpdateCentralPhysical, src/solver.cpp:155-159).  The faces only ask for
+// cells the central lines hold.
 MPD_HD Phys central_phys(const BcView &v, int l, int m) {
+    int idx;
+    const int line = central_line(v.g.L, v.g.M, l, m, idx);
     double u[8];
-    if (m == v.g.M && (l == 1 || l == v.g.L)) {
-        const double *s = v.snap + (l == 1 ? 0 : 8);
+    if (line >= 0) {
+        const double *b = v.cphys + (size_t)line * 8 * v.len + idx;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) u[k] = s[k];
-    } else {
-        load_cons(v.u, v.g.ps, v.g.ix(l, m), u);
+        for (int k = 0; k < 8; ++k) u[k] = b[(size_t)k * v.len];
+        return recon_exact(u, v.g.r(l, m), v.g.gamma);
     }
+    load_cons(v.u, v.g.ps, v.g.ix(l, m), u);
     return recon_exact(u, v.g.r(l, m), v.g.gamma);
 }
 

@@ -1,0 +1,255 @@
+// TMA-staged interior kernel of the plain FP64 path (MPD_PRECISION_FAST).
+//
+// The arithmetic is lf_fast.cuh's (FastStrip::eval / point, fast_finish), so
+// the result is bit-identical to it; what changes is how the rows arrive and
+// how the work is spread:
+//   * a warp owns a strip of 32 point columns starting at an even column
+//     x0 = 30 s (30 output cells, lanes 0 and 31 are halo points) and a band
+//     of rows; the rows it needs are fetched by one TMA tile load each
+//     ({32 columns} x {1 row} x {8 conserved planes} = 2 KB) into a ring of
+//     kTmaStages shared-memory stages, kTmaStages - 1 rows ahead of use, so a
+//     warp keeps several rows in flight without holding them in registers;
+//   * the launch is one wave: bands are sized so that strips x bands equals
+//     the number of warps the GPU holds at once, instead of a fixed band
+//     height that leaves a partial second wave.
+// Rows outside the planes (l = -1, l = L+2) and columns past M+2 arrive as
+// zeros (TMA out-of-bounds fill); ghost rows and columns are zero in memory.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "lf_fast.cuh"
+#include "tma.cuh"
+
+namespace mpd {
+
+// Build-time tuning: resident blocks per SM the register budget is cut for,
+// and staged rows per warp.
+#ifndef MPD_TMA_MINB
+#define MPD_TMA_MINB 3
+#endif
+#ifndef MPD_TMA_STAGES
+#define MPD_TMA_STAGES 4
+#endif
+
+constexpr int kTmaWarps = 4;                  // warps per block
+constexpr int kTmaStages = MPD_TMA_STAGES;    // rows in flight per warp
+constexpr int kTmaRow = 8 * 32;               // doubles per staged row
+constexpr int kTmaRowBytes = kTmaRow * 8;     // 2048
+// + 128 bytes to align the stages: TMA destinations need 128-byte alignment
+constexpr int kTmaSmem = kTmaWarps * kTmaStages * (kTmaRowBytes + 8) + 128;
+
+// Rows [l_begin, l_end) of band b out of nbands over l = 1..L.
+__host__ __device__ inline void tma_band(int L, int nbands, int b, int &l_begin, int &l_end) {
+    l_begin = 1 + (int)((long long)b * L / nbands);
+    l_end = 1 + (int)((long long)(b + 1) * L / nbands);
+}
+
+struct TmaWarp {
+    FastStrip f;
+    const CUtensorMap *map;
+    double *stage;   // kTmaStages rows of [8][32]
+    uint32_t bar0;   // shared address of this warp's first barrier
+    int row0;        // plane row of staged row j = 0
+    int nrows;       // rows this warp stages
+    int lane;
+
+    __device__ __forceinline__ uint32_t bar(int s) const { return bar0 + 8u * (uint32_t)s; }
+
+    __device__ __forceinline__ void issue(int j) const {
+        if (lane == 0 && j < nrows) {
+            const int s = j % kTmaStages;
+            mbar_expect_tx(bar(s), kTmaRowBytes);
+            tma_load_3d(smem_addr(stage + s * kTmaRow), map, bar(s), f.p - lane, row0 + j, 0);
+        }
+    }
+
+    // Staged row j into U (zeros on columns past M+1); false if the wait gave up.
+    __device__ __forceinline__ bool take(int j, double U[8]) const {
+        const int s = j % kTmaStages;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar(s), (j / kTmaStages) & 1));
+        const double *src = stage + s * kTmaRow + lane;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) U[k] = f.pvalid ? src[32 * k] : 0.0;
+        return ok;
+    }
+
+    // Row j's values are in registers and used: refill its stage with row j + kTmaStages.
+    __device__ __forceinline__ void release(int j) const {
+        __syncwarp();
+        issue(j + kTmaStages);
+    }
+};
+
+template <bool WANT_WS>
+__device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, int l_end, int &j, double Acur[9],
+                                        double B[9], unsigned long long &ws_key, unsigned int &nf) {
+    const FastStrip &s = w.f;
+    const int n = l + 1;  // point row n closes cell row l
+    double Un[8];
+    if (!w.take(j, Un)) return false;
+    FastPrim q;
+    double r, Gz[8], out[8];
+    const bool gh = s.eval(n, Un, q, r, Gz);
+    w.release(j);
+    ++j;
+    fast_finish(Acur, B, Un, Gz, s.kz, out);
+    if (s.out_lane) {
+        const Geo &g = s.g;
+        const size_t i = g.ix(l, s.p);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s.u[(size_t)k * g.ps + i] = out[k];
+        if (wants_central(g.L, g.M, l, s.p))
+            store_central(s.cphys, s.len, g.L, g.M, l, s.p, out);
+        if (WANT_WS && l >= 2 && l <= g.L - 1) {
+            const double wsp = fast_wave_speed(out, s.radius(l), g.gamma);
+            if (!isfinite(wsp)) nf = 1u;
+            const unsigned long long kk = max_key(wsp, nf);
+            ws_key = kk > ws_key ? kk : ws_key;
+        }
+    }
+    if (n < l_end) s.point(n, Un, q, r, Gz, gh, true, Acur, B);
+    return true;
+}
+
+template <bool WANT_WS>
+__global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
+    lf_tma_kernel(Geo g, const __grid_constant__ CUtensorMap map0,
+                  const __grid_constant__ CUtensorMap map1, double *buf0, double *buf1,
+                  DevState *st, double dt_arg, int use_state_dt, double *cphys, int len,
+                  int nstrips, int nbands) {
+    extern __shared__ __align__(128) unsigned char tma_smem_raw[];
+    unsigned char *tma_smem = tma_smem_raw + ((128u - (smem_addr(tma_smem_raw) & 127u)) & 127u);
+    if (st->done) return;
+    const long long step = st->step;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int task = (int)blockIdx.x * kTmaWarps + wib;
+    const int strip = task % nstrips;
+    const int band = task / nstrips;
+
+    TmaWarp w;
+    FastStrip &s = w.f;
+    s.g = g;
+    s.u = (step & 1) ? buf0 : buf1;
+    s.st = st;
+    s.cphys = cphys;
+    s.len = len;
+    s.dt = use_state_dt ? st->dt : dt_arg;
+    s.p = kFastCells * strip + lane;
+    s.pvalid = s.p <= g.M + 1;
+    s.out_lane = lane >= 1 && lane <= kFastCells && s.p >= 2 && s.p <= g.M;
+    s.frac = (double)(s.p - 1) * g.dy;
+    s.gm1 = g.gamma - 1.0;
+    s.kz = s.dt * (0.5 / g.dz);
+    w.map = (step & 1) ? &map1 : &map0;
+    w.stage = reinterpret_cast<double *>(tma_smem) + wib * kTmaStages * kTmaRow;
+    w.bar0 = smem_addr(tma_smem + kTmaWarps * kTmaStages * kTmaRowBytes) + 8u * wib * kTmaStages;
+    w.lane = lane;
+
+    unsigned long long ws_key = 0ull;
+    unsigned int nf = 0u;
+    int l_begin = 1, l_end = 1;
+    if (band < nbands) tma_band(g.L, nbands, band, l_begin, l_end);
+    if (l_begin < l_end) {
+        w.row0 = l_begin - 1;
+        w.nrows = l_end - l_begin + 2;
+        if (lane == 0) {
+            tmap_prefetch(w.map);
+            for (int k = 0; k < kTmaStages; ++k) mbar_init(w.bar(k), 1);
+            mbar_init_fence();
+        }
+        __syncwarp();
+        for (int k = 0; k < kTmaStages; ++k) w.issue(k);
+
+        bool ok = true;
+        int j = 0;
+        double A0[9], A1[9], B[9], U[8], Gz[8], r;
+        FastPrim q;
+        ok = w.take(j, U);
+        if (ok) {
+            bool gh = s.eval(l_begin - 1, U, q, r, Gz);
+            w.release(j);
+            ++j;
+            s.point(l_begin - 1, U, q, r, Gz, gh, false, A0, B);  // A of the first cell row
+            ok = w.take(j, U);
+            if (ok) {
+                gh = s.eval(l_begin, U, q, r, Gz);
+                w.release(j);
+                ++j;
+                s.point(l_begin, U, q, r, Gz, gh, true, A1, B);    // its B, and A of the next
+            }
+        }
+        int l = l_begin;
+        // two rows per trip so the A buffers swap roles without copies
+        for (; ok && l + 1 < l_end; l += 2) {
+            ok = tma_row<WANT_WS>(w, l, l_end, j, A0, B, ws_key, nf);
+            if (ok) ok = tma_row<WANT_WS>(w, l + 1, l_end, j, A1, B, ws_key, nf);
+        }
+        if (ok && l < l_end) ok = tma_row<WANT_WS>(w, l, l_end, j, A0, B, ws_key, nf);
+        if (!ok) {
+            // a row never arrived: let the copies still in flight land (bounded),
+            // record the failure and stop the run
+            if (lane == 0) {
+                for (int jj = j; jj < w.nrows && jj < j + kTmaStages; ++jj)
+                    mbar_wait_bounded(w.bar(jj % kTmaStages), (jj / kTmaStages) & 1);
+                atomicExch(&st->wait_fail, 1);
+                atomicExch(&st->done, 1);
+            }
+            __syncwarp();
+        }
+    }
+    if (WANT_WS) {
+        unsigned long long key[1] = {ws_key};
+        unsigned long long *dst[1] = {&st->ws_acc};
+        block_max_atomic<1>(key, nf, dst, &st->nf_acc);
+    }
+}
+
+// Strips and bands for one wave of lf_tma_kernel on this device.
+struct TmaPlan {
+    int nstrips = 0, nbands = 0, blocks = 0;
+};
+
+inline cudaError_t plan_lf_tma(const Geo &g, int device, TmaPlan &plan) {
+    int sms = 0, per_sm = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(lf_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kTmaSmem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(lf_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kTmaSmem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lf_tma_kernel<true>,
+                                                      32 * kTmaWarps, kTmaSmem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const int warps = sms * per_sm * kTmaWarps;
+    plan.nstrips = (g.M + kFastCells - 1) / kFastCells;
+    int nb = warps / plan.nstrips;
+    const int min_band = 4;  // rows; each band re-reads two rows above its first
+    if (nb > g.L / min_band) nb = g.L / min_band;
+    if (nb < 1) nb = 1;
+    plan.nbands = nb;
+    const int tasks = plan.nstrips * plan.nbands;
+    plan.blocks = (tasks + kTmaWarps - 1) / kTmaWarps;
+    return cudaSuccess;
+}
+
+inline void launch_lf_tma(const Geo &g, const TmaPlan &plan, const CUtensorMap &map0,
+                          const CUtensorMap &map1, double *buf0, double *buf1, DevState *st,
+                          double dt, int use_state_dt, bool want_ws, double *cphys, int len,
+                          cudaStream_t stream) {
+    if (want_ws)
+        lf_tma_kernel<true><<<plan.blocks, 32 * kTmaWarps, kTmaSmem, stream>>>(
+            g, map0, map1, buf0, buf1, st, dt, use_state_dt, cphys, len, plan.nstrips,
+            plan.nbands);
+    else
+        lf_tma_kernel<false><<<plan.blocks, 32 * kTmaWarps, kTmaSmem, stream>>>(
+            g, map0, map1, buf0, buf1, st, dt, use_state_dt, cphys, len, plan.nstrips,
+            plan.nbands);
+}
+
+}  // namespace mpd

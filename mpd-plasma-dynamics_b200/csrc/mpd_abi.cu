@@ -13,6 +13,7 @@
 #include "bc_compile.hpp"
 #include "kernels.cuh"
 #include "lf_fast.cuh"
+#include "lf_tma.cuh"
 
 namespace mpd {
 namespace {
@@ -39,6 +40,44 @@ int Fail(int code, const std::string &msg) {
     } while (0)
 
 constexpr int kRedBlocks = 592;  // 4 x 148 SMs for the deterministic sums
+constexpr int kBcBlock = 64;     // boundary-ring threads per block
+
+// cuTensorMapEncodeTiled, fetched from the driver at run time (no -lcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn GetEncodeTiled() {
+    static EncodeTiledFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return static_cast<EncodeTiledFn>(nullptr);
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// The 8 conserved planes of one state buffer as a 3-D tensor
+// {columns M+3, rows L+2, planes 8} with the row pitch and plane stride of the
+// allocation; tiles are {32 columns, 1 row, 8 planes}, zero-filled outside.
+int EncodeStateMap(CUtensorMap *map, double *base, int cols, int rows, int pitch, size_t ps) {
+    EncodeTiledFn enc = GetEncodeTiled();
+    if (!enc) return Fail(MPD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable from the driver");
+    const cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, 8};
+    const cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(double), (cuuint64_t)ps * sizeof(double)};
+    const cuuint32_t box[3] = {32, 1, 8};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return Fail(MPD_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return MPD_OK;
+}
 
 }  // namespace
 
@@ -52,6 +91,11 @@ struct mpd_solver {
     double *buf[2] = {nullptr, nullptr};
     double *ic = nullptr, *prev = nullptr, *geo = nullptr, *stage = nullptr;
     double *partials = nullptr, *small = nullptr;
+    double *cphys = nullptr;                 // central lines (boundary inputs)
+    double *wall[2] = {nullptr, nullptr};    // wall lines, by step parity
+    int len = 0;                             // line length
+    CUtensorMap tmap[2];                     // conserved planes of buf[0] / buf[1]
+    mpd::TmaPlan plan;                       // one-wave strips x bands
     unsigned long long *red = nullptr;
     mpd::DevState *st = nullptr;
     mpd::DevState *h_st = nullptr;  // pinned mirror
@@ -63,7 +107,7 @@ struct mpd_solver {
     int with_prev = 0;
     long long host_step = 0;
     cudaGraphExec_t graph = nullptr;
-    int graph_steps = 0, graph_check = 0;
+    int graph_steps = 0, graph_check = 0, graph_resid = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, snap_ev = nullptr, stage_ev = nullptr;
     bool snap_pending = false;
     size_t dev_bytes = 0;
@@ -91,6 +135,9 @@ void FreeAll(mpd_solver *s) {
     cudaFree(s->geo);
     cudaFree(s->stage);
     cudaFree(s->partials);
+    cudaFree(s->cphys);
+    cudaFree(s->wall[0]);
+    cudaFree(s->wall[1]);
     cudaFree(s->small);
     cudaFree(s->red);
     cudaFree(s->st);
@@ -133,6 +180,13 @@ int UploadPhysical(mpd_solver *s, const double *phys10) {
     MPD_CK(cudaMemsetAsync(s->buf[1], 0, 8 * s->ps * sizeof(double), s->stream));
     mpd::init_conservative_kernel<<<4 * 148, 256, 0, s->stream>>>(s->g, s->ic, s->buf[0]);
     MPD_CK(cudaGetLastError());
+    const size_t line_bytes = static_cast<size_t>(10) * s->len * sizeof(double);
+    MPD_CK(cudaMemsetAsync(s->cphys, 0, mpd::kCentralLines * 8 * s->len * sizeof(double),
+                           s->stream));
+    MPD_CK(cudaMemsetAsync(s->wall[1], 0, mpd::kWallLines * line_bytes, s->stream));
+    mpd::init_wall_kernel<<<(s->rows + 127) / 128, 128, 0, s->stream>>>(s->g, s->ic, s->wall[0],
+                                                                          s->len);
+    MPD_CK(cudaGetLastError());
     if (s->with_prev) {
         // Fields::SavePrev after initialisation (src/main.cpp:150-152)
         const int from[7] = {mpd::P_RHO, mpd::P_VZ, mpd::P_VR, mpd::P_VPHI,
@@ -154,30 +208,53 @@ int UploadPhysical(mpd_solver *s, const double *phys10) {
     return MPD_OK;
 }
 
-// One time step: interior kernel, boundary kernel (+ controller), and in run
-// mode the guarded relative-L2 convergence check.
-int EnqueueStep(mpd_solver *s, bool first, bool use_state_dt, double dt, bool with_check) {
+// One time step: interior kernel, boundary kernel (+ controller), in run mode
+// the guarded relative-L2 convergence check and, every residual_every steps,
+// the L-inf residual.  want_ws: fuse the maximum wave speed (adaptive dt and
+// the per-call ComputeDt need it).
+int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool want_ws) {
     const mpd::Geo &g = s->g;
+    const int usd = use_state_dt ? 1 : 0;
     if (first || s->precision == MPD_PRECISION_EXACT) {
         dim3 block(32, 8);
         dim3 grid((g.M - 1 + 31) / 32, (g.L + 7) / 8);
         if (first)
             mpd::lf_exact_kernel<true><<<grid, block, 0, s->stream>>>(
-                g, s->buf[0], s->buf[1], s->ic, s->st, dt, use_state_dt ? 1 : 0);
+                g, s->buf[0], s->buf[1], s->ic, s->st, dt, usd, s->cphys, s->len);
         else
             mpd::lf_exact_kernel<false><<<grid, block, 0, s->stream>>>(
-                g, s->buf[0], s->buf[1], s->ic, s->st, dt, use_state_dt ? 1 : 0);
+                g, s->buf[0], s->buf[1], s->ic, s->st, dt, usd, s->cphys, s->len);
     } else {
-        mpd::launch_lf_fast(g, s->buf[0], s->buf[1], s->st, dt, use_state_dt ? 1 : 0, s->stream);
+        mpd::launch_lf_tma(g, s->plan, s->tmap[0], s->tmap[1], s->buf[0], s->buf[1], s->st, dt,
+                           usd, want_ws, s->cphys, s->len, s->stream);
     }
     MPD_CK(cudaGetLastError());
-    const int nring = mpd::ring_count(g);
-    mpd::bc_kernel<<<(nring + 127) / 128, 128, 0, s->stream>>>(
-        g, s->buf[0], s->buf[1], s->ic, s->bc, s->st, dt, use_state_dt ? 1 : 0);
+    return MPD_OK;
+}
+
+int LaunchBoundary(mpd_solver *s, bool use_state_dt, double dt) {
+    const int nring = mpd::ring_count(s->g);
+    mpd::bc_kernel<<<(nring + kBcBlock - 1) / kBcBlock, kBcBlock, 0, s->stream>>>(
+        s->g, s->buf[0], s->buf[1], s->ic, s->bc, s->st, dt, use_state_dt ? 1 : 0, s->cphys,
+        s->wall[0], s->wall[1], s->len);
     MPD_CK(cudaGetLastError());
+    return MPD_OK;
+}
+
+int EnqueueStep(mpd_solver *s, bool first, bool use_state_dt, double dt, bool with_check,
+                bool want_ws, bool with_residual) {
+    const mpd::Geo &g = s->g;
+    int rc = LaunchInterior(s, first, use_state_dt, dt, want_ws);
+    if (rc != MPD_OK) return rc;
+    rc = LaunchBoundary(s, use_state_dt, dt);
+    if (rc != MPD_OK) return rc;
     if (with_check) {
         mpd::change_kernel<<<kRedBlocks, 256, 0, s->stream>>>(Bufs(s), s->prev, s->partials, 1, 1);
         mpd::change_finish_kernel<<<1, 32, 0, s->stream>>>(s->partials, kRedBlocks, s->st, 1);
+        MPD_CK(cudaGetLastError());
+    }
+    if (with_residual) {
+        mpd::residual_kernel<<<kRedBlocks, 256, 0, s->stream>>>(g, s->buf[0], s->buf[1], s->st);
         MPD_CK(cudaGetLastError());
     }
     return MPD_OK;
@@ -187,6 +264,8 @@ int SyncState(mpd_solver *s) {
     MPD_CK(cudaMemcpyAsync(s->h_st, s->st, sizeof(mpd::DevState), cudaMemcpyDeviceToHost,
                            s->stream));
     MPD_CK(cudaStreamSynchronize(s->stream));
+    if (s->h_st->wait_fail)
+        return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
     return MPD_OK;
 }
 
@@ -203,8 +282,10 @@ int CheckHandle(mpd_solver *s) {
     return MPD_OK;
 }
 
-int BuildGraph(mpd_solver *s, int steps, bool with_check) {
-    if (s->graph && s->graph_steps == steps && s->graph_check == (with_check ? 1 : 0))
+int BuildGraph(mpd_solver *s, int steps, bool with_check, bool want_ws, int resid_every) {
+    const int key = (with_check ? 1 : 0) | (want_ws ? 2 : 0);
+    if (s->graph && s->graph_steps == steps && s->graph_check == key &&
+        s->graph_resid == resid_every)
         return MPD_OK;
     if (s->graph) {
         cudaGraphExecDestroy(s->graph);
@@ -213,7 +294,10 @@ int BuildGraph(mpd_solver *s, int steps, bool with_check) {
     cudaGraph_t graph = nullptr;
     MPD_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     int rc = MPD_OK;
-    for (int i = 0; i < steps && rc == MPD_OK; ++i) rc = EnqueueStep(s, false, true, 0.0, with_check);
+    for (int i = 0; i < steps && rc == MPD_OK; ++i) {
+        const bool res = resid_every > 0 && (i + 1) % resid_every == 0;
+        rc = EnqueueStep(s, false, true, 0.0, with_check, want_ws, res);
+    }
     const cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
     if (rc != MPD_OK) {
         if (graph) cudaGraphDestroy(graph);
@@ -224,7 +308,8 @@ int BuildGraph(mpd_solver *s, int steps, bool with_check) {
     cudaGraphDestroy(graph);
     if (e2 != cudaSuccess) return Fail(MPD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2));
     s->graph_steps = steps;
-    s->graph_check = with_check ? 1 : 0;
+    s->graph_check = key;
+    s->graph_resid = resid_every;
     return MPD_OK;
 }
 
@@ -284,6 +369,10 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     if (s->with_prev) STEP(DevAlloc(s, &s->prev, 7 * s->ps));
     STEP(DevAlloc(s, &s->geo, 5 * static_cast<size_t>(s->rows)));
     STEP(DevAlloc(s, &s->partials, static_cast<size_t>(kRedBlocks) * 8));
+    s->len = mpd::line_len(s->L, s->M);
+    STEP(DevAlloc(s, &s->cphys, static_cast<size_t>(mpd::kCentralLines) * 8 * s->len));
+    STEP(DevAlloc(s, &s->wall[0], static_cast<size_t>(mpd::kWallLines) * 10 * s->len));
+    STEP(DevAlloc(s, &s->wall[1], static_cast<size_t>(mpd::kWallLines) * 10 * s->len));
     STEP(DevAlloc(s, &s->small, 16));
     STEP(DevAlloc(s, &s->red, 4));
     STEP(DevAlloc(s, &s->st, 1));
@@ -324,6 +413,14 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     g.drin = s->geo + 2 * s->rows;
     g.drout = s->geo + 3 * s->rows;
     g.dr = s->geo + 4 * s->rows;
+    if (s->precision == MPD_PRECISION_FAST) {
+        for (int b = 0; b < 2; ++b)
+            STEP(EncodeStateMap(&s->tmap[b], s->buf[b], s->cols, s->rows, s->pitch, s->ps));
+        if (mpd::plan_lf_tma(g, s->device, s->plan) != cudaSuccess) {
+            FreeAll(s);
+            return Fail(MPD_ERR_CUDA, "occupancy query for the interior kernel failed");
+        }
+    }
     // boundary table
     STEP(DevAlloc(s, &s->d_seg, cbc.seg.size() ? cbc.seg.size() : 1));
     STEP(DevAlloc(s, &s->d_code, cbc.code.size()));
@@ -345,6 +442,9 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     s->bc.seg = s->d_seg;
     s->bc.code = s->d_code;
     s->bc.consts = s->d_consts;
+    s->bc.nseg_total = static_cast<int>(cbc.seg.size());
+    s->bc.ncode = static_cast<int>(cbc.code.size());
+    s->bc.nconst = static_cast<int>(cbc.consts.size());
     STEP(UploadPhysical(s, phys10));
 #undef STEP
     *out = s;
@@ -360,7 +460,7 @@ void mpd_destroy(mpd_solver *s) {
 int mpd_advance(mpd_solver *s, double dt) {
     int rc = CheckHandle(s);
     if (rc != MPD_OK) return rc;
-    rc = EnqueueStep(s, s->host_step == 0, false, dt, false);
+    rc = EnqueueStep(s, s->host_step == 0, false, dt, false, true, false);
     if (rc != MPD_OK) return rc;
     s->host_step++;
     return MPD_OK;
@@ -375,7 +475,10 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
     if (p->convergence_threshold > 0.0 && p->check_frequency <= 0)
         return Fail(MPD_ERR_INVALID, "check_frequency must be positive");
     if (p->max_steps <= 0) return Fail(MPD_ERR_INVALID, "max_steps must be positive");
+    if (p->residual_every < 0 || p->residual_every > 4096)
+        return Fail(MPD_ERR_INVALID, "residual_every must be in [0, 4096]");
     const bool with_check = p->convergence_threshold > 0.0;
+    const bool want_ws = p->adaptive != 0;
     rc = SyncState(s);
     if (rc != MPD_OK) return rc;
     mpd::DevState &h = *s->h_st;
@@ -406,20 +509,26 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
 
     MPD_CK(cudaEventRecord(s->ev0, s->stream));
     if (!h.done && s->host_step == 0) {
-        rc = EnqueueStep(s, true, true, 0.0, with_check);
+        rc = EnqueueStep(s, true, true, 0.0, with_check, want_ws, p->residual_every == 1);
         if (rc != MPD_OK) return rc;
     }
+    // Steps per graph launch: a multiple of the residual interval, so that the
+    // residual is evaluated every residual_every steps.
     int per_graph = p->steps_per_graph > 0 ? p->steps_per_graph : 100;
     if (with_check && p->check_frequency > 0 && per_graph % p->check_frequency != 0 &&
         p->check_frequency < per_graph)
         per_graph = (per_graph / p->check_frequency) * p->check_frequency;
-    rc = BuildGraph(s, per_graph, with_check);
+    if (p->residual_every > 0 && per_graph % p->residual_every != 0)
+        per_graph = (per_graph / p->residual_every + 1) * p->residual_every;
+    rc = BuildGraph(s, per_graph, with_check, want_ws, p->residual_every);
     if (rc != MPD_OK) return rc;
     long long last_step = -1;
     for (;;) {
         MPD_CK(cudaMemcpyAsync(s->h_st, s->st, sizeof(mpd::DevState), cudaMemcpyDeviceToHost,
                                s->stream));
         MPD_CK(cudaStreamSynchronize(s->stream));
+        if (h.wait_fail)
+            return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
         if (h.done) break;
         if (h.step == last_step)  // a launch that advanced nothing: stop, don't spin
             return Fail(MPD_ERR_TIMEOUT, "run loop made no progress");
@@ -430,13 +539,18 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
     MPD_CK(cudaEventSynchronize(s->ev1));
     float ms = 0.f;
     MPD_CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    // the residual of the final state, when the loop stopped between checks
+    if (!h.resid_valid && h.step > 0) {
+        mpd::residual_kernel<<<kRedBlocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st);
+        MPD_CK(cudaGetLastError());
+    }
     rc = SyncState(s);
     if (rc != MPD_OK) return rc;
     if (stats) {
         stats->steps = h.step - step0;
         stats->t = h.t;
         stats->dt = h.dt;
-        stats->residual = h.last_resid;
+        stats->residual = h.resid_valid ? h.last_resid : NAN;
         stats->change = h.last_change;
         stats->max_wave_speed = h.last_ws;
         stats->converged = h.converged;
@@ -555,9 +669,11 @@ int mpd_residual(mpd_solver *s, double *out) {
     int rc = CheckHandle(s);
     if (rc != MPD_OK) return rc;
     if (!out) return Fail(MPD_ERR_INVALID, "out is NULL");
+    mpd::residual_kernel<<<kRedBlocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st);
+    MPD_CK(cudaGetLastError());
     rc = SyncState(s);
     if (rc != MPD_OK) return rc;
-    *out = s->h_st->resid_valid ? s->h_st->last_resid : NAN;
+    *out = (s->h_st->step > 0 && s->h_st->resid_valid) ? s->h_st->last_resid : NAN;
     return MPD_OK;
 }
 
@@ -676,40 +792,34 @@ int mpd_profile_kernels(mpd_solver *s, int steps, double dt, double out_ms[2]) {
     int rc = CheckHandle(s);
     if (rc != MPD_OK) return rc;
     if (steps <= 0 || !out_ms) return Fail(MPD_ERR_INVALID, "bad profile request");
-    cudaEvent_t ev[3];
+    // all launches are queued before any is waited for, so each event pair
+    // brackets device work only (no host launch gap inside a pair)
+    std::vector<cudaEvent_t> ev(3 * static_cast<size_t>(steps), nullptr);
     for (auto &e : ev) MPD_CK(cudaEventCreate(&e));
-    double tot[2] = {0.0, 0.0};
-    const mpd::Geo &g = s->g;
-    for (int i = 0; i < steps; ++i) {
+    for (int i = 0; i < steps && rc == MPD_OK; ++i) {
         const bool first = s->host_step == 0;
-        MPD_CK(cudaEventRecord(ev[0], s->stream));
-        if (first || s->precision == MPD_PRECISION_EXACT) {
-            dim3 block(32, 8);
-            dim3 grid((g.M - 1 + 31) / 32, (g.L + 7) / 8);
-            if (first)
-                mpd::lf_exact_kernel<true><<<grid, block, 0, s->stream>>>(g, s->buf[0], s->buf[1],
-                                                                           s->ic, s->st, dt, 0);
-            else
-                mpd::lf_exact_kernel<false><<<grid, block, 0, s->stream>>>(g, s->buf[0], s->buf[1],
-                                                                            s->ic, s->st, dt, 0);
-        } else {
-            mpd::launch_lf_fast(g, s->buf[0], s->buf[1], s->st, dt, 0, s->stream);
-        }
-        MPD_CK(cudaEventRecord(ev[1], s->stream));
-        const int nring = mpd::ring_count(g);
-        mpd::bc_kernel<<<(nring + 127) / 128, 128, 0, s->stream>>>(g, s->buf[0], s->buf[1], s->ic,
-                                                                   s->bc, s->st, dt, 0);
-        MPD_CK(cudaEventRecord(ev[2], s->stream));
-        MPD_CK(cudaGetLastError());
-        MPD_CK(cudaEventSynchronize(ev[2]));
-        float a = 0.f, b = 0.f;
-        MPD_CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
-        MPD_CK(cudaEventElapsedTime(&b, ev[1], ev[2]));
-        tot[0] += a;
-        tot[1] += b;
+        MPD_CK(cudaEventRecord(ev[3 * i], s->stream));
+        rc = LaunchInterior(s, first, false, dt, true);
+        if (rc != MPD_OK) break;
+        MPD_CK(cudaEventRecord(ev[3 * i + 1], s->stream));
+        rc = LaunchBoundary(s, false, dt);
+        if (rc != MPD_OK) break;
+        MPD_CK(cudaEventRecord(ev[3 * i + 2], s->stream));
         s->host_step++;
     }
+    double tot[2] = {0.0, 0.0};
+    if (rc == MPD_OK) {
+        MPD_CK(cudaStreamSynchronize(s->stream));
+        for (int i = 0; i < steps; ++i) {
+            float a = 0.f, b = 0.f;
+            MPD_CK(cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]));
+            MPD_CK(cudaEventElapsedTime(&b, ev[3 * i + 1], ev[3 * i + 2]));
+            tot[0] += a;
+            tot[1] += b;
+        }
+    }
     for (auto &e : ev) cudaEventDestroy(e);
+    if (rc != MPD_OK) return rc;
     out_ms[0] = tot[0] / steps;
     out_ms[1] = tot[1] / steps;
     return MPD_OK;

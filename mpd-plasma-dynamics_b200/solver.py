@@ -94,11 +94,18 @@ class GpuSolver:
         self._call("mpd_advance", float(dt))
 
     def run(self, T: float = float("inf"), dt: float | None = None, adaptive: bool | None = None,
-            max_steps: int = 1 << 40, residual_tol: float = 0.0, residual_every: int = 1,
+            max_steps: int = 1 << 40, residual_tol: float = 0.0, residual_every: int | None = None,
             convergence_threshold: float | None = None, check_frequency: int | None = None,
             steps_per_graph: int = 0) -> RunResult:
-        """Graph-resident driver loop (src/main.cpp:191-282)."""
+        """Graph-resident driver loop (src/main.cpp:191-282).
+
+        The L-inf residual (a separate pass over both state buffers) is
+        evaluated every ``residual_every`` steps: by default every 50 steps
+        when ``residual_tol`` is set, otherwise only for the final state.
+        """
         cfg = self.cfg
+        if residual_every is None:
+            residual_every = 50 if residual_tol > 0.0 else 0
         p = N.RunParams()
         p.T = T
         p.dt = cfg.dt if dt is None else dt
