@@ -208,7 +208,10 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(solver.stream_handle())
 
     # warm-up (includes the exact first step and the graph build)
-    solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=max(args.warmup, 1))
+    # one graph of exactly --warmup steps, so no launch in the profile is an
+    # early exit of a graph that ran past the step limit
+    w = max(args.warmup, 1)
+    solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=w, steps_per_graph=w)
     _, step0 = solver.time()
     dt_now = solver.ComputeDt(cfg.dt)
 
@@ -317,7 +320,10 @@ def run_profile(args):
     case = _case()
     cfg = case.cfg
     solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision=args.precision)
-    solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=max(args.warmup, 1))
+    # one graph of exactly --warmup steps, so no launch in the profile is an
+    # early exit of a graph that ran past the step limit
+    w = max(args.warmup, 1)
+    solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=w, steps_per_graph=w)
     dt = solver.ComputeDt(cfg.dt)
     for _ in range(args.steps):
         solver.Advance(dt)

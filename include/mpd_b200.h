@@ -114,6 +114,15 @@ int mpd_advance(mpd_solver *s, double dt);
  * (Diagnostics::ComputeDt after every step), the reference's relative-L2
  * convergence check every check_frequency steps, and an L-inf residual
  * criterion.  Runs until t >= T, convergence, or max_steps. */
+/* How mpd_run drives the steps.  GRAPH: an interior and a boundary kernel per
+ * step, replayed from captured CUDA graphs.  PERSISTENT: one cooperative
+ * launch runs many steps with grid barriers between the interior and the
+ * boundary phase (fast precision, no SolutionChange checks).  AUTO takes
+ * GRAPH.  Both give the same results, bit for bit. */
+#define MPD_ENGINE_AUTO 0
+#define MPD_ENGINE_GRAPH 1
+#define MPD_ENGINE_PERSISTENT 2
+
 typedef struct mpd_run_params {
     double T;                   /* end time (use a huge value for step-limited runs) */
     double dt;                  /* initial dt (SimConfig::dt)                         */
@@ -125,6 +134,7 @@ typedef struct mpd_run_params {
     int residual_every;           /* steps between residual evaluations (>= 1)       */
     long long max_steps;
     int steps_per_graph;          /* steps captured per CUDA graph launch (0 = auto) */
+    int engine;                   /* MPD_ENGINE_AUTO / _GRAPH / _PERSISTENT           */
 } mpd_run_params;
 
 typedef struct mpd_run_stats {

@@ -31,6 +31,7 @@ STATUS_NAMES = {
 
 FACE_L_LO, FACE_L_HI, FACE_M_LO, FACE_M_HI = 0, 1, 2, 3
 NEUMANN, DIRICHLET, EXPRESSION, AXIS_LF = 0, 1, 2, 3
+ENGINE_AUTO, ENGINE_GRAPH, ENGINE_PERSISTENT = 0, 1, 2
 PRECISION_EXACT, PRECISION_FAST = 0, 1
 PHYS_FIELDS = ("rho", "v_z", "v_r", "v_phi", "e", "p", "P", "H_z", "H_r", "H_phi")
 
@@ -66,7 +67,8 @@ class RunParams(C.Structure):
                 ("dt_min", C.c_double), ("dt_max", C.c_double),
                 ("convergence_threshold", C.c_double), ("check_frequency", C.c_int),
                 ("residual_tol", C.c_double), ("residual_every", C.c_int),
-                ("max_steps", C.c_longlong), ("steps_per_graph", C.c_int)]
+                ("max_steps", C.c_longlong), ("steps_per_graph", C.c_int),
+                ("engine", C.c_int)]
 
 
 class RunStats(C.Structure):

@@ -65,6 +65,83 @@ void EvalOrder(const mpd_bc_segment &s, const mpd_field_cond *out[8]) {
     out[Q_E] = &s.e;
 }
 
+// Symbols that are the same in every cell: their values are known here.
+bool CellIndependent(int sym) {
+    return sym == BS_GAMMA || sym == BS_BETA || sym == BS_HZ0 || sym == BS_R0 || sym == BS_DZ;
+}
+
+double CellIndependentValue(const mpd_config &cfg, int sym) {
+    switch (sym) {
+        case BS_GAMMA: return cfg.gamma;
+        case BS_BETA: return cfg.beta;
+        case BS_HZ0: return cfg.H_z0;
+        case BS_R0: return cfg.r_0;
+        default: return cfg.dz;
+    }
+}
+
+// Closed form of a compiled expression (SegDesc::form and operands of field
+// j).  Folding evaluates the same IEEE operations in the same order as the
+// interpreter would, so every form gives the interpreter's bits.
+void ClosedForm(const mpd_config &cfg, const ExprCode &ec, int j, SegDesc &d) {
+    d.form[j] = EF_GENERAL;
+    d.fa[j] = d.fb[j] = -1;
+    d.ca[j] = d.cb[j] = 0.0;
+    d.fop[j] = OP_MUL;
+    bool foldable = true;
+    for (int32_t ins : ec.code) {
+        const int op = ins & 0xff;
+        const int arg = ins >> 8;
+        const bool arith = op == OP_END || op == OP_CONST || op == OP_NEG || op == OP_ADD ||
+                           op == OP_SUB || op == OP_MUL || op == OP_DIV;
+        if (!(arith || (op == OP_VAR && CellIndependent(arg)))) foldable = false;
+    }
+    if (foldable) {
+        double sym[BS_COUNT];
+        for (int t = 0; t < BS_COUNT; ++t) sym[t] = CellIndependent(t) ? CellIndependentValue(cfg, t) : NAN;
+        d.form[j] = EF_CONST;
+        d.ca[j] = eval_code(ec.code.data(), ec.consts.data(), sym);
+        return;
+    }
+    // operand: a symbol (cell-independent ones become constants) or a constant
+    auto operand = [&](int32_t ins, int &sym, double &c) {
+        const int op = ins & 0xff;
+        const int arg = ins >> 8;
+        if (op == OP_CONST) {
+            sym = -1;
+            c = ec.consts[arg];
+            return true;
+        }
+        if (op != OP_VAR) return false;
+        if (CellIndependent(arg)) {
+            sym = -1;
+            c = CellIndependentValue(cfg, arg);
+        } else {
+            sym = arg;
+        }
+        return true;
+    };
+    const std::vector<int32_t> &c = ec.code;
+    if (c.size() == 2 && (c[1] & 0xff) == OP_END && operand(c[0], d.fa[j], d.ca[j])) {
+        // x * 1.0 is x exactly
+        d.form[j] = EF_BIN;
+        d.fop[j] = OP_MUL;
+        d.fb[j] = -1;
+        d.cb[j] = 1.0;
+        return;
+    }
+    if (c.size() == 4 && (c[3] & 0xff) == OP_END) {
+        const int op = c[2] & 0xff;
+        if ((op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV) &&
+            operand(c[0], d.fa[j], d.ca[j]) && operand(c[1], d.fb[j], d.cb[j])) {
+            d.form[j] = EF_BIN;
+            d.fop[j] = op;
+            return;
+        }
+    }
+    d.fa[j] = d.fb[j] = -1;
+}
+
 }  // namespace
 
 int CompileBc(const mpd_config &cfg, CompiledBc &out, std::string &err) {
@@ -141,6 +218,7 @@ int CompileBc(const mpd_config &cfg, CompiledBc &out, std::string &err) {
                         return MPD_ERR_UNSUPPORTED_BC;
                     }
                 }
+                ClosedForm(cfg, ec, j, d);
                 // relocate constants into the shared pool
                 const int cbase = static_cast<int>(out.consts.size());
                 out.consts.insert(out.consts.end(), ec.consts.begin(), ec.consts.end());

@@ -190,6 +190,7 @@ int mpd_emu_advance(void *h, double dt, int order) {
     v.wphys = s->wall[s->step & 1].data();
     v.len = s->len;
     v.first = first ? 1 : 0;
+    v.fast = s->precision == MPD_PRECISION_FAST ? 1 : 0;
     v.dt = dt;
     v.bc = s->bc;
     const int nring = mpd::ring_count(g);
@@ -202,7 +203,7 @@ int mpd_emu_advance(void *h, double dt, int order) {
         mpd::bc_ring_final(v, l, m, uf);
         if (m == 1 || m == g.M + 1)
             mpd::store_line_phys(s->wall[(s->step + 1) & 1].data(), s->len, m == 1 ? 0 : 1, l,
-                                 mpd::recon_exact(uf, g.r(l, m), g.gamma));
+                                 mpd::recon_bc(v, uf, g.r(l, m)));
         if (order != 0)
             for (int k = 0; k < 8; ++k) u[k * g.ps + g.ix(l, m)] = uf[k];
     }

@@ -106,6 +106,28 @@ struct CellStats {
     }
 };
 
+// Boundary-ring cell i of one step: its final conserved values into v.u, and
+// the full reconstruction of the cell: its wave speed (want_ws) and, for the
+// wall columns, the "old" value the next step's faces read (wall lines wnext).
+__device__ __forceinline__ void ring_cell_update(const BcView &v, int i, double *wnext,
+                                                 bool want_ws, CellStats &cs) {
+    const Geo &g = v.g;
+    int l, m;
+    ring_cell(g, i, l, m);
+    double uf[8];
+    bc_ring_final(v, l, m, uf);
+    const size_t ix = g.ix(l, m);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v.u[(size_t)k * g.ps + ix] = uf[k];
+    const bool wall = m == 1 || m == g.M + 1;
+    if (want_ws || wall) {
+        const double r = g.r(l, m);
+        const Phys q = recon_bc(v, uf, r);
+        if (want_ws) cs.add_ws(v.fast ? fast_wave_speed(uf, r, g.gamma) : wave_speed(q, g.gamma));
+        if (wall) store_line_phys(wnext, v.len, m == 1 ? 0 : 1, l, q);
+    }
+}
+
 // Exact interior update (Solver::ComputeCentralUpdate + the implicit
 // UpdatePhysicalFromU of the neighbours), one thread per cell
 // l in [1, L], m in [2, M].  FIRST: the stencil reads the initial physical
@@ -160,28 +182,13 @@ __global__ void __launch_bounds__(64) bc_kernel(Geo g, double *buf0, double *buf
                                                  const double *__restrict__ ic, BcTable bc,
                                                  DevState *st, double dt_arg, int use_state_dt,
                                                  const double *cphys, double *wall0, double *wall1,
-                                                 int len) {
+                                                 int len, int fast) {
     if (st->done) return;
     const long long step = st->step;
     const double *u0 = (step & 1) ? buf1 : buf0;
     double *u = (step & 1) ? buf0 : buf1;
     const double dt = use_state_dt ? st->dt : dt_arg;
     const int flags = step_flags(st);
-    // the boundary table is read many times per thread: stage it in shared memory
-    __shared__ SegDesc s_seg[kMaxSegments];
-    __shared__ int32_t s_code[kSmemCode];
-    __shared__ double s_const[kSmemConst];
-    {
-        const int nwords = bc.nseg_total * (int)(sizeof(SegDesc) / sizeof(int));
-        const int *src = reinterpret_cast<const int *>(bc.seg);
-        int *dst = reinterpret_cast<int *>(s_seg);
-        for (int w = threadIdx.x; w < nwords; w += blockDim.x) dst[w] = src[w];
-        if (bc.ncode <= kSmemCode)
-            for (int w = threadIdx.x; w < bc.ncode; w += blockDim.x) s_code[w] = bc.code[w];
-        if (bc.nconst <= kSmemConst)
-            for (int w = threadIdx.x; w < bc.nconst; w += blockDim.x) s_const[w] = bc.consts[w];
-        __syncthreads();
-    }
     BcView v;
     v.g = g;
     v.u0 = u0;
@@ -191,32 +198,14 @@ __global__ void __launch_bounds__(64) bc_kernel(Geo g, double *buf0, double *buf
     v.wphys = (step & 1) ? wall1 : wall0;
     v.len = len;
     v.first = step == 0;
+    v.fast = fast;
     v.dt = dt;
     v.bc = bc;
-    v.bc.seg = s_seg;
-    if (bc.ncode <= kSmemCode) v.bc.code = s_code;
-    if (bc.nconst <= kSmemConst) v.bc.consts = s_const;
     double *wnext = (step & 1) ? wall0 : wall1;
     CellStats cs;
     cs.init();
     const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    if (i < ring_count(g)) {
-        int l, m;
-        ring_cell(g, i, l, m);
-        double uf[8];
-        bc_ring_final(v, l, m, uf);
-        const size_t ix = g.ix(l, m);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) u[(size_t)k * g.ps + ix] = uf[k];
-        const bool wall = m == 1 || m == g.M + 1;
-        if ((flags & kFlagWs) || wall) {
-            // the full reconstruction of this cell: wave speed, and for the
-            // wall columns the "old" value the next step's faces read
-            const Phys q = recon_exact(uf, g.r(l, m), g.gamma);
-            if (flags & kFlagWs) cs.add_ws(wave_speed(q, g.gamma));
-            if (wall) store_line_phys(wnext, len, m == 1 ? 0 : 1, l, q);
-        }
-    }
+    if (i < ring_count(g)) ring_cell_update(v, i, wnext, (flags & kFlagWs) != 0, cs);
     if (flags) cs.flush(st);
 
     // ---- last block: finalise the step -------------------------------------

@@ -19,8 +19,10 @@
 
 #ifdef __CUDACC__
 #define MPD_HD __host__ __device__ __forceinline__
+#define MPD_HD_NOINLINE __host__ __device__ __noinline__
 #else
 #define MPD_HD inline
+#define MPD_HD_NOINLINE inline
 #endif
 
 #include "expr_ops.h"
@@ -447,6 +449,11 @@ MPD_HD double eval_code(const int32_t *code, const double *consts, const double 
 // One segment, compiled: local inclusive range along the face's free axis
 // after FaceBC::Apply's sentinel resolution, ClipToLocal and the M_LO corner
 // policy (src/face_bc.cpp:104-129); conditions in evaluation order.
+// Closed forms of expression fields, found by the host compiler: a folded
+// constant, or one binary operation on two operands (symbols or constants).
+// Anything else runs through the bytecode interpreter.
+enum ExprForm { EF_GENERAL = 0, EF_CONST = 1, EF_BIN = 2 };
+
 struct SegDesc {
     int lo, hi;
     int has_axis;
@@ -454,6 +461,10 @@ struct SegDesc {
     int type[8];
     int code[8];      // offset of the expression's bytecode, -1 if none
     double value[8];
+    int form[8];      // ExprForm of an expression field
+    int fop[8];       // OP_ADD / OP_SUB / OP_MUL / OP_DIV for EF_BIN
+    int fa[8], fb[8]; // operand symbols (BcSym), -1 for a constant operand
+    double ca[8], cb[8];  // constant operands; ca is the value of EF_CONST
 };
 
 struct BcTable {
@@ -465,22 +476,16 @@ struct BcTable {
     int nseg_total, ncode, nconst;
 };
 
-// Largest expression code / constant pools the boundary kernel stages in
-// shared memory (larger tables are read from global memory).
-constexpr int kSmemCode = 1024;
-constexpr int kSmemConst = 256;
-
-// Everything one boundary step reads.
-// Physical values of the cells the boundary faces read, laid out as "lines"
-// of 10 fields (Phys order) along one grid row or column: line stride
-// 10 * len, field stride len.
+// Values of the cells the boundary faces read, laid out as "lines" along one
+// grid row or column (field stride len).
 //   central lines (the interior kernel's new conserved values, 8 fields, of
 //   the cells the faces read; the boundary kernel reconstructs them):
 //   0 = row 2 by m, 1 = row L-1 by m, 2 = column 2 by l, 3 = column M by l
 //   (its entries l = 1 and l = L are (1,M) and (L,M) before the L faces
 //   overwrite them);
-//   wall lines (the previous step's full reconstruction of the wall columns,
-//   written by the boundary kernel; the initial condition on step 0):
+//   wall lines (10 physical fields in Phys order, line stride 10 * len: the
+//   previous step's full reconstruction of the wall columns, written by the
+//   boundary kernel; the initial condition on step 0):
 //   0 = column 1 by l, 1 = column M+1 by l.
 constexpr int kCentralLines = 4;
 constexpr int kWallLines = 2;
@@ -554,9 +559,29 @@ struct BcView {
     const double *wphys;  // wall lines at the start of this step
     int len;              // line length
     int first;            // step 0: "old" physical values are the IC planes
+    int fast;             // MPD_PRECISION_FAST: reconstruct with reciprocals
     double dt;
     BcTable bc;
 };
+
+// Fields::UpdatePhysicalFromU of one cell on the boundary path: the exact
+// divides in exact mode, the interior kernel's reciprocal form in fast mode.
+MPD_HD Phys recon_bc(const BcView &v, const double u[8], double r) {
+    if (!v.fast) return recon_exact(u, r, v.g.gamma);
+    const FastPrim f = fast_prim(u, r, v.g.gamma - 1.0);
+    Phys q;
+    q.rho = f.rho;
+    q.vz = f.vz;
+    q.vr = f.vr;
+    q.vphi = f.vphi;
+    q.e = f.e;
+    q.p = f.p;
+    q.P = f.P;
+    q.Hz = f.Hz;
+    q.Hr = f.Hr;
+    q.Hphi = f.Hphi;
+    return q;
+}
 
 // Primitive values in evaluation order.
 struct Prim {
@@ -586,7 +611,7 @@ MPD_HD Phys old_phys(const BcView &v, int l, int m) {
     if (v.first) return load_phys(v.ic, v.g.ps, i);
     double u[8];
     load_cons(v.u0, v.g.ps, i, u);
-    return recon_exact(u, v.g.r(l, m), v.g.gamma);
+    return recon_bc(v, u, v.g.r(l, m));
 }
 
 // Physical value of a central cell after this step's central update
@@ -600,10 +625,10 @@ MPD_HD Phys central_phys(const BcView &v, int l, int m) {
         const double *b = v.cphys + (size_t)line * 8 * v.len + idx;
 #pragma unroll
         for (int k = 0; k < 8; ++k) u[k] = b[(size_t)k * v.len];
-        return recon_exact(u, v.g.r(l, m), v.g.gamma);
+        return recon_bc(v, u, v.g.r(l, m));
     }
     load_cons(v.u, v.g.ps, v.g.ix(l, m), u);
-    return recon_exact(u, v.g.r(l, m), v.g.gamma);
+    return recon_bc(v, u, v.g.r(l, m));
 }
 
 // Last segment of `face` whose range covers free index k, or -1.
@@ -616,52 +641,91 @@ MPD_HD int last_cover(const BcView &v, int face, int k, int limit) {
     return -1;
 }
 
+// Value of boundary expression symbol `idx` at cell (l, m) with neighbour
+// (ln, mn); out holds the fields already evaluated in this cell.
+MPD_HD double bc_sym(const BcView &v, int idx, int l, int m, int ln, int mn, const Prim &nb,
+                     const Prim &out) {
+    switch (idx) {
+        case BS_GAMMA: return v.g.gamma;
+        case BS_BETA: return v.g.beta;
+        case BS_HZ0: return v.g.H_z0;
+        case BS_R0: return v.g.r_0;
+        case BS_DZ: return v.g.dz;
+        case BS_DR: return v.g.dr[l];
+        case BS_R: return v.g.r(l, m);
+        case BS_RZ: return v.g.rz(l, m);
+        case BS_Z: return (double)(l - 1) * v.g.dz;
+        case BS_RNB: return v.g.r(ln, mn);
+        case BS_RZNB: return v.g.rz(ln, mn);
+        // *_nb symbols in the reference's SetNeighbors order:
+        // rho, v_z, v_r, v_phi, e, H_z, H_r, H_phi
+        case BS_NB0 + 0: return nb.v[Q_RHO];
+        case BS_NB0 + 1: return nb.v[Q_VZ];
+        case BS_NB0 + 2: return nb.v[Q_VR];
+        case BS_NB0 + 3: return nb.v[Q_VPHI];
+        case BS_NB0 + 4: return nb.v[Q_E];
+        case BS_NB0 + 5: return nb.v[Q_HZ];
+        case BS_NB0 + 6: return nb.v[Q_HR];
+        case BS_NB0 + 7: return nb.v[Q_HPHI];
+        case BS_CUR0 + 0: return out.v[0];
+        case BS_CUR0 + 1: return out.v[1];
+        case BS_CUR0 + 2: return out.v[2];
+        case BS_CUR0 + 3: return out.v[3];
+        case BS_CUR0 + 4: return out.v[4];
+        case BS_CUR0 + 5: return out.v[5];
+        case BS_CUR0 + 6: return out.v[6];
+        case BS_CUR0 + 7: return out.v[7];
+        default: return NAN;
+    }
+}
+
+// An expression field the closed forms don't cover: full symbol table and
+// the bytecode interpreter.  Kept out of line so the common path stays small
+// and free of indexed local arrays.
+MPD_HD_NOINLINE double bc_eval_general(const BcView &v, int code, int l, int m, int ln, int mn,
+                                       Prim nb, Prim out) {
+    double sym[BS_COUNT];
+    for (int t = 0; t < BS_COUNT; ++t) sym[t] = bc_sym(v, t, l, m, ln, mn, nb, out);
+    return eval_code(v.bc.code + code, v.bc.consts, sym);
+}
+
+MPD_HD double bc_binop(int op, double a, double b) {
+    switch (op) {
+        case OP_ADD: return a + b;
+        case OP_SUB: return a - b;
+        case OP_MUL: return a * b;
+        default: return a / b;
+    }
+}
+
 // PerFieldBC::Apply's per-cell field evaluation (src/bcs/per_field_bc.cpp:
 // 286-292 resolve, 311-360 / 393-446 expression path): writes the 8 new
 // primitives of cell (l, m) given its neighbour's primitives and the values
 // to keep (AxisLF fields keep the cell's current value).
 MPD_HD void eval_segment(const BcView &v, const SegDesc &d, int l, int m, int ln, int mn,
                          const Prim &nb, const Prim &keep, Prim &out) {
-    double sym[BS_COUNT];
-    bool have_sym = false;
+#pragma unroll 1
     for (int j = 0; j < 8; ++j) {
         double val;
         switch (d.type[j]) {
             case COND_NEUMANN: val = nb.v[j] + d.value[j]; break;
             case COND_DIRICHLET: val = d.value[j]; break;
             case COND_EXPR: {
-                if (!have_sym) {
-                    have_sym = true;
-                    sym[BS_GAMMA] = v.g.gamma;
-                    sym[BS_BETA] = v.g.beta;
-                    sym[BS_HZ0] = v.g.H_z0;
-                    sym[BS_R0] = v.g.r_0;
-                    sym[BS_DZ] = v.g.dz;
-                    sym[BS_DR] = v.g.dr[l];
-                    sym[BS_R] = v.g.r(l, m);
-                    sym[BS_RZ] = v.g.rz(l, m);
-                    sym[BS_Z] = (double)(l - 1) * v.g.dz;
-                    sym[BS_RNB] = v.g.r(ln, mn);
-                    sym[BS_RZNB] = v.g.rz(ln, mn);
-                    // *_nb symbols in the reference's SetNeighbors order:
-                    // rho, v_z, v_r, v_phi, e, H_z, H_r, H_phi
-                    sym[BS_NB0 + 0] = nb.v[Q_RHO];
-                    sym[BS_NB0 + 1] = nb.v[Q_VZ];
-                    sym[BS_NB0 + 2] = nb.v[Q_VR];
-                    sym[BS_NB0 + 3] = nb.v[Q_VPHI];
-                    sym[BS_NB0 + 4] = nb.v[Q_E];
-                    sym[BS_NB0 + 5] = nb.v[Q_HZ];
-                    sym[BS_NB0 + 6] = nb.v[Q_HR];
-                    sym[BS_NB0 + 7] = nb.v[Q_HPHI];
-                    for (int t = 0; t < j; ++t) sym[BS_CUR0 + t] = out.v[t];
+                const int form = d.form[j];
+                if (form == EF_CONST) {
+                    val = d.ca[j];
+                } else if (form == EF_BIN) {
+                    const double a = d.fa[j] < 0 ? d.ca[j] : bc_sym(v, d.fa[j], l, m, ln, mn, nb, out);
+                    const double b = d.fb[j] < 0 ? d.cb[j] : bc_sym(v, d.fb[j], l, m, ln, mn, nb, out);
+                    val = bc_binop(d.fop[j], a, b);
+                } else {
+                    val = bc_eval_general(v, d.code[j], l, m, ln, mn, nb, out);
                 }
-                val = eval_code(v.bc.code + d.code[j], v.bc.consts, sym);
                 break;
             }
             default: val = keep.v[j]; break;
         }
         out.v[j] = val;
-        if (have_sym) sym[BS_CUR0 + j] = val;
     }
 }
 

@@ -51,23 +51,36 @@ struct TmaWarp {
     const CUtensorMap *map;
     double *stage;   // kTmaStages rows of [8][32]
     uint32_t bar0;   // shared address of this warp's first barrier
-    int row0;        // plane row of staged row j = 0
-    int nrows;       // rows this warp stages
+    uint32_t jbase;  // running row count at the band's first staged row
+    int row0;        // plane row of the band's first staged row
+    int nrows;       // rows the band stages
     int lane;
 
-    __device__ __forceinline__ uint32_t bar(int s) const { return bar0 + 8u * (uint32_t)s; }
+    __device__ __forceinline__ uint32_t bar(uint32_t s) const { return bar0 + 8u * s; }
 
-    __device__ __forceinline__ void issue(int j) const {
-        if (lane == 0 && j < nrows) {
-            const int s = j % kTmaStages;
+    // Barriers of this warp's stages; once per launch, before the first issue.
+    __device__ __forceinline__ void init() const {
+        if (lane == 0) {
+            tmap_prefetch(map);
+            for (int k = 0; k < kTmaStages; ++k) mbar_init(bar(k), 1);
+            mbar_init_fence();
+        }
+        __syncwarp();
+    }
+
+    // Staged row j (running count) of the band: one TMA tile load into stage j % kTmaStages.
+    __device__ __forceinline__ void issue(uint32_t j) const {
+        if (lane == 0 && j - jbase < (uint32_t)nrows) {
+            const uint32_t s = j % kTmaStages;
             mbar_expect_tx(bar(s), kTmaRowBytes);
-            tma_load_3d(smem_addr(stage + s * kTmaRow), map, bar(s), f.p - lane, row0 + j, 0);
+            tma_load_3d(smem_addr(stage + s * kTmaRow), map, bar(s), f.p - lane,
+                        row0 + (int)(j - jbase), 0);
         }
     }
 
     // Staged row j into U (zeros on columns past M+1); false if the wait gave up.
-    __device__ __forceinline__ bool take(int j, double U[8]) const {
-        const int s = j % kTmaStages;
+    __device__ __forceinline__ bool take(uint32_t j, double U[8]) const {
+        const uint32_t s = j % kTmaStages;
         const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar(s), (j / kTmaStages) & 1));
         const double *src = stage + s * kTmaRow + lane;
 #pragma unroll
@@ -76,15 +89,16 @@ struct TmaWarp {
     }
 
     // Row j's values are in registers and used: refill its stage with row j + kTmaStages.
-    __device__ __forceinline__ void release(int j) const {
+    __device__ __forceinline__ void release(uint32_t j) const {
         __syncwarp();
         issue(j + kTmaStages);
     }
 };
 
 template <bool WANT_WS>
-__device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, int l_end, int &j, double Acur[9],
-                                        double B[9], unsigned long long &ws_key, unsigned int &nf) {
+__device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, int l_end, uint32_t &j,
+                                        double Acur[9], double B[9], unsigned long long &ws_key,
+                                        unsigned int &nf) {
     const FastStrip &s = w.f;
     const int n = l + 1;  // point row n closes cell row l
     double Un[8];
@@ -100,8 +114,7 @@ __device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, int l_end, int 
         const size_t i = g.ix(l, s.p);
 #pragma unroll
         for (int k = 0; k < 8; ++k) s.u[(size_t)k * g.ps + i] = out[k];
-        if (wants_central(g.L, g.M, l, s.p))
-            store_central(s.cphys, s.len, g.L, g.M, l, s.p, out);
+        if (wants_central(g.L, g.M, l, s.p)) store_central(s.cphys, s.len, g.L, g.M, l, s.p, out);
         if (WANT_WS && l >= 2 && l <= g.L - 1) {
             const double wsp = fast_wave_speed(out, s.radius(l), g.gamma);
             if (!isfinite(wsp)) nf = 1u;
@@ -113,6 +126,79 @@ __device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, int l_end, int 
     return true;
 }
 
+// Cell rows [l_begin, l_end) of the warp's strip.  j is the running staged-row
+// count (advanced by the l_end - l_begin + 2 rows the band consumes).  Returns
+// false if a row never arrived; the copies still in flight have then been
+// waited for (bounded).
+template <bool WANT_WS>
+__device__ __forceinline__ bool tma_band_run(TmaWarp &w, int l_begin, int l_end, uint32_t &j,
+                                             unsigned long long &ws_key, unsigned int &nf) {
+    const FastStrip &s = w.f;
+    w.row0 = l_begin - 1;
+    w.nrows = l_end - l_begin + 2;
+    w.jbase = j;
+    for (int k = 0; k < kTmaStages; ++k) w.issue(j + k);
+    bool ok;
+    double A0[9], A1[9], B[9], U[8], Gz[8], r;
+    FastPrim q;
+    ok = w.take(j, U);
+    if (ok) {
+        bool gh = s.eval(l_begin - 1, U, q, r, Gz);
+        w.release(j);
+        ++j;
+        s.point(l_begin - 1, U, q, r, Gz, gh, false, A0, B);  // A of the first cell row
+        ok = w.take(j, U);
+        if (ok) {
+            gh = s.eval(l_begin, U, q, r, Gz);
+            w.release(j);
+            ++j;
+            s.point(l_begin, U, q, r, Gz, gh, true, A1, B);    // its B, and A of the next
+        }
+    }
+    int l = l_begin;
+    // two rows per trip so the A buffers swap roles without copies
+    for (; ok && l + 1 < l_end; l += 2) {
+        ok = tma_row<WANT_WS>(w, l, l_end, j, A0, B, ws_key, nf);
+        if (ok) ok = tma_row<WANT_WS>(w, l + 1, l_end, j, A1, B, ws_key, nf);
+    }
+    if (ok && l < l_end) ok = tma_row<WANT_WS>(w, l, l_end, j, A0, B, ws_key, nf);
+    if (!ok) {
+        if (w.lane == 0) {
+            const uint32_t end = w.jbase + (uint32_t)w.nrows;
+            for (uint32_t jj = j; jj < end && jj < j + kTmaStages; ++jj)
+                mbar_wait_bounded(w.bar(jj % kTmaStages), (jj / kTmaStages) & 1);
+        }
+        __syncwarp();
+    }
+    return ok;
+}
+
+// Strip, lanes and per-step constants of warp `task`'s FastStrip.
+__device__ __forceinline__ void tma_warp_setup(TmaWarp &w, const Geo &g, int strip, double *u,
+                                               DevState *st, double *cphys, int len, double dt,
+                                               const CUtensorMap *map) {
+    FastStrip &s = w.f;
+    const int lane = threadIdx.x & 31;
+    s.g = g;
+    s.u = u;
+    s.st = st;
+    s.cphys = cphys;
+    s.len = len;
+    s.dt = dt;
+    s.p = kFastCells * strip + lane;
+    s.pvalid = s.p <= g.M + 1;
+    s.out_lane = lane >= 1 && lane <= kFastCells && s.p >= 2 && s.p <= g.M;
+    s.frac = (double)(s.p - 1) * g.dy;
+    s.gm1 = g.gamma - 1.0;
+    s.kz = dt * (0.5 / g.dz);
+    w.map = map;
+    w.lane = lane;
+}
+
+__device__ __forceinline__ unsigned char *tma_smem_base(unsigned char *raw) {
+    return raw + ((128u - (smem_addr(raw) & 127u)) & 127u);
+}
+
 template <bool WANT_WS>
 __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
     lf_tma_kernel(Geo g, const __grid_constant__ CUtensorMap map0,
@@ -120,84 +206,31 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
                   DevState *st, double dt_arg, int use_state_dt, double *cphys, int len,
                   int nstrips, int nbands) {
     extern __shared__ __align__(128) unsigned char tma_smem_raw[];
-    unsigned char *tma_smem = tma_smem_raw + ((128u - (smem_addr(tma_smem_raw) & 127u)) & 127u);
+    unsigned char *tma_smem = tma_smem_base(tma_smem_raw);
     if (st->done) return;
     const long long step = st->step;
-    const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int task = (int)blockIdx.x * kTmaWarps + wib;
     const int strip = task % nstrips;
     const int band = task / nstrips;
 
     TmaWarp w;
-    FastStrip &s = w.f;
-    s.g = g;
-    s.u = (step & 1) ? buf0 : buf1;
-    s.st = st;
-    s.cphys = cphys;
-    s.len = len;
-    s.dt = use_state_dt ? st->dt : dt_arg;
-    s.p = kFastCells * strip + lane;
-    s.pvalid = s.p <= g.M + 1;
-    s.out_lane = lane >= 1 && lane <= kFastCells && s.p >= 2 && s.p <= g.M;
-    s.frac = (double)(s.p - 1) * g.dy;
-    s.gm1 = g.gamma - 1.0;
-    s.kz = s.dt * (0.5 / g.dz);
-    w.map = (step & 1) ? &map1 : &map0;
+    tma_warp_setup(w, g, strip, (step & 1) ? buf0 : buf1, st, cphys, len,
+                   use_state_dt ? st->dt : dt_arg, (step & 1) ? &map1 : &map0);
     w.stage = reinterpret_cast<double *>(tma_smem) + wib * kTmaStages * kTmaRow;
     w.bar0 = smem_addr(tma_smem + kTmaWarps * kTmaStages * kTmaRowBytes) + 8u * wib * kTmaStages;
-    w.lane = lane;
 
     unsigned long long ws_key = 0ull;
     unsigned int nf = 0u;
     int l_begin = 1, l_end = 1;
     if (band < nbands) tma_band(g.L, nbands, band, l_begin, l_end);
     if (l_begin < l_end) {
-        w.row0 = l_begin - 1;
-        w.nrows = l_end - l_begin + 2;
-        if (lane == 0) {
-            tmap_prefetch(w.map);
-            for (int k = 0; k < kTmaStages; ++k) mbar_init(w.bar(k), 1);
-            mbar_init_fence();
-        }
-        __syncwarp();
-        for (int k = 0; k < kTmaStages; ++k) w.issue(k);
-
-        bool ok = true;
-        int j = 0;
-        double A0[9], A1[9], B[9], U[8], Gz[8], r;
-        FastPrim q;
-        ok = w.take(j, U);
-        if (ok) {
-            bool gh = s.eval(l_begin - 1, U, q, r, Gz);
-            w.release(j);
-            ++j;
-            s.point(l_begin - 1, U, q, r, Gz, gh, false, A0, B);  // A of the first cell row
-            ok = w.take(j, U);
-            if (ok) {
-                gh = s.eval(l_begin, U, q, r, Gz);
-                w.release(j);
-                ++j;
-                s.point(l_begin, U, q, r, Gz, gh, true, A1, B);    // its B, and A of the next
-            }
-        }
-        int l = l_begin;
-        // two rows per trip so the A buffers swap roles without copies
-        for (; ok && l + 1 < l_end; l += 2) {
-            ok = tma_row<WANT_WS>(w, l, l_end, j, A0, B, ws_key, nf);
-            if (ok) ok = tma_row<WANT_WS>(w, l + 1, l_end, j, A1, B, ws_key, nf);
-        }
-        if (ok && l < l_end) ok = tma_row<WANT_WS>(w, l, l_end, j, A0, B, ws_key, nf);
-        if (!ok) {
-            // a row never arrived: let the copies still in flight land (bounded),
-            // record the failure and stop the run
-            if (lane == 0) {
-                for (int jj = j; jj < w.nrows && jj < j + kTmaStages; ++jj)
-                    mbar_wait_bounded(w.bar(jj % kTmaStages), (jj / kTmaStages) & 1);
-                atomicExch(&st->wait_fail, 1);
-                atomicExch(&st->done, 1);
-            }
-            __syncwarp();
+        w.init();
+        uint32_t j = 0;
+        if (!tma_band_run<WANT_WS>(w, l_begin, l_end, j, ws_key, nf) && w.lane == 0) {
+            // a row never arrived: record the failure and stop the run
+            atomicExch(&st->wait_fail, 1);
+            atomicExch(&st->done, 1);
         }
     }
     if (WANT_WS) {

@@ -13,6 +13,7 @@
 #include "bc_compile.hpp"
 #include "kernels.cuh"
 #include "lf_fast.cuh"
+#include "lf_persist.cuh"
 #include "lf_tma.cuh"
 
 namespace mpd {
@@ -96,6 +97,9 @@ struct mpd_solver {
     int len = 0;                             // line length
     CUtensorMap tmap[2];                     // conserved planes of buf[0] / buf[1]
     mpd::TmaPlan plan;                       // one-wave strips x bands
+    mpd::TmaPlan pplan;                      // persistent launch (cooperative wave)
+    bool persist_ok = false;                 // the persistent engine can run here
+    mpd::GridSync *gsync = nullptr;          // its barrier and reduction words
     unsigned long long *red = nullptr;
     mpd::DevState *st = nullptr;
     mpd::DevState *h_st = nullptr;  // pinned mirror
@@ -136,6 +140,7 @@ void FreeAll(mpd_solver *s) {
     cudaFree(s->stage);
     cudaFree(s->partials);
     cudaFree(s->cphys);
+    cudaFree(s->gsync);
     cudaFree(s->wall[0]);
     cudaFree(s->wall[1]);
     cudaFree(s->small);
@@ -236,7 +241,7 @@ int LaunchBoundary(mpd_solver *s, bool use_state_dt, double dt) {
     const int nring = mpd::ring_count(s->g);
     mpd::bc_kernel<<<(nring + kBcBlock - 1) / kBcBlock, kBcBlock, 0, s->stream>>>(
         s->g, s->buf[0], s->buf[1], s->ic, s->bc, s->st, dt, use_state_dt ? 1 : 0, s->cphys,
-        s->wall[0], s->wall[1], s->len);
+        s->wall[0], s->wall[1], s->len, s->precision == MPD_PRECISION_FAST ? 1 : 0);
     MPD_CK(cudaGetLastError());
     return MPD_OK;
 }
@@ -420,6 +425,10 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
             FreeAll(s);
             return Fail(MPD_ERR_CUDA, "occupancy query for the interior kernel failed");
         }
+        // the persistent engine needs cooperative launch and a strip per warp
+        s->persist_ok = mpd::plan_lf_persist(g, s->device, s->pplan) == cudaSuccess;
+        cudaGetLastError();
+        if (s->persist_ok) STEP(DevAlloc(s, &s->gsync, 1));
     }
     // boundary table
     STEP(DevAlloc(s, &s->d_seg, cbc.seg.size() ? cbc.seg.size() : 1));
@@ -463,6 +472,47 @@ int mpd_advance(mpd_solver *s, double dt) {
     rc = EnqueueStep(s, s->host_step == 0, false, dt, false, true, false);
     if (rc != MPD_OK) return rc;
     s->host_step++;
+    return MPD_OK;
+}
+
+// End of mpd_run: device time, the final residual, stats, and back to per-call mode.
+static int FinishRun(mpd_solver *s, long long step0, mpd_run_stats *stats) {
+    mpd::DevState &h = *s->h_st;
+    int rc = MPD_OK;
+    MPD_CK(cudaEventRecord(s->ev1, s->stream));
+    MPD_CK(cudaEventSynchronize(s->ev1));
+    float ms = 0.f;
+    MPD_CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    // the residual of the final state, when the loop stopped between checks
+    if (!h.resid_valid && h.step > 0) {
+        mpd::residual_kernel<<<kRedBlocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st);
+        MPD_CK(cudaGetLastError());
+    }
+    rc = SyncState(s);
+    if (rc != MPD_OK) return rc;
+    if (stats) {
+        stats->steps = h.step - step0;
+        stats->t = h.t;
+        stats->dt = h.dt;
+        stats->residual = h.resid_valid ? h.last_resid : NAN;
+        stats->change = h.last_change;
+        stats->max_wave_speed = h.last_ws;
+        stats->converged = h.converged;
+        stats->status = h.nonfinite ? MPD_ERR_NONFINITE : MPD_OK;
+        stats->device_ms = ms;
+    }
+    s->host_step = h.step;
+    const bool nonfinite = h.nonfinite != 0;
+    // back to drop-in (per-call) mode
+    h.run_mode = 0;
+    h.done = 0;
+    h.want_ws = 1;
+    h.resid_every = 1;
+    h.T = INFINITY;
+    h.max_steps = LLONG_MAX;
+    rc = PushState(s);
+    if (rc != MPD_OK) return rc;
+    if (nonfinite) return Fail(MPD_ERR_NONFINITE, "non-finite value in the state");
     return MPD_OK;
 }
 
@@ -512,6 +562,46 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
         rc = EnqueueStep(s, true, true, 0.0, with_check, want_ws, p->residual_every == 1);
         if (rc != MPD_OK) return rc;
     }
+    if (p->engine == MPD_ENGINE_PERSISTENT && (!s->persist_ok || with_check))
+        return Fail(MPD_ERR_INVALID,
+                    "the persistent engine needs fast precision, cooperative launch and no "
+                    "convergence_threshold");
+    // AUTO takes the graph path: on the measured workloads it is the faster one
+    // (the persistent engine pays two grid barriers per step and runs the
+    // boundary chains of every face inside one phase)
+    if (p->engine == MPD_ENGINE_PERSISTENT) {
+        // one cooperative launch per chunk of steps; the residual keeps the
+        // graph path's schedule: after steps (step - base) % residual_every == 0
+        mpd::PersistArgs a{};
+        a.g = s->g;
+        a.buf0 = s->buf[0];
+        a.buf1 = s->buf[1];
+        a.cphys = s->cphys;
+        a.wall0 = s->wall[0];
+        a.wall1 = s->wall[1];
+        a.len = s->len;
+        a.bc = s->bc;
+        a.st = s->st;
+        a.gs = s->gsync;
+        a.nstrips = s->pplan.nstrips;
+        a.nbands = s->pplan.nbands;
+        a.nsteps = 2000;
+        a.resid_base = step0 + ((!h.done && s->host_step == 0) ? 1 : 0);
+        long long last = -1;
+        for (;;) {
+            MPD_CK(cudaMemcpyAsync(s->h_st, s->st, sizeof(mpd::DevState), cudaMemcpyDeviceToHost,
+                                   s->stream));
+            MPD_CK(cudaStreamSynchronize(s->stream));
+            if (h.wait_fail)
+                return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
+            if (h.done) break;
+            if (h.step == last) return Fail(MPD_ERR_TIMEOUT, "run loop made no progress");
+            last = h.step;
+            MPD_CK(cudaMemsetAsync(s->gsync, 0, sizeof(mpd::GridSync), s->stream));
+            MPD_CK(mpd::launch_lf_persist(s->pplan, s->tmap[0], s->tmap[1], a, s->stream));
+        }
+        return FinishRun(s, step0, stats);
+    }
     // Steps per graph launch: a multiple of the residual interval, so that the
     // residual is evaluated every residual_every steps.
     int per_graph = p->steps_per_graph > 0 ? p->steps_per_graph : 100;
@@ -535,41 +625,7 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
         last_step = h.step;
         MPD_CK(cudaGraphLaunch(s->graph, s->stream));
     }
-    MPD_CK(cudaEventRecord(s->ev1, s->stream));
-    MPD_CK(cudaEventSynchronize(s->ev1));
-    float ms = 0.f;
-    MPD_CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
-    // the residual of the final state, when the loop stopped between checks
-    if (!h.resid_valid && h.step > 0) {
-        mpd::residual_kernel<<<kRedBlocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st);
-        MPD_CK(cudaGetLastError());
-    }
-    rc = SyncState(s);
-    if (rc != MPD_OK) return rc;
-    if (stats) {
-        stats->steps = h.step - step0;
-        stats->t = h.t;
-        stats->dt = h.dt;
-        stats->residual = h.resid_valid ? h.last_resid : NAN;
-        stats->change = h.last_change;
-        stats->max_wave_speed = h.last_ws;
-        stats->converged = h.converged;
-        stats->status = h.nonfinite ? MPD_ERR_NONFINITE : MPD_OK;
-        stats->device_ms = ms;
-    }
-    s->host_step = h.step;
-    const bool nonfinite = h.nonfinite != 0;
-    // back to drop-in (per-call) mode
-    h.run_mode = 0;
-    h.done = 0;
-    h.want_ws = 1;
-    h.resid_every = 1;
-    h.T = INFINITY;
-    h.max_steps = LLONG_MAX;
-    rc = PushState(s);
-    if (rc != MPD_OK) return rc;
-    if (nonfinite) return Fail(MPD_ERR_NONFINITE, "non-finite value in the state");
-    return MPD_OK;
+    return FinishRun(s, step0, stats);
 }
 
 int mpd_max_wave_speed(mpd_solver *s, double *out) {

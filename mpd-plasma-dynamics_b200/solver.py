@@ -20,6 +20,7 @@ from .geometry import GeometryRegistry, Grid
 from .ic import ArrayIC, ExpressionIC, IInitialCondition
 
 PRECISIONS = {"exact": N.PRECISION_EXACT, "fast": N.PRECISION_FAST}
+ENGINES = {"auto": N.ENGINE_AUTO, "graph": N.ENGINE_GRAPH, "persistent": N.ENGINE_PERSISTENT}
 
 
 @dataclasses.dataclass
@@ -96,12 +97,15 @@ class GpuSolver:
     def run(self, T: float = float("inf"), dt: float | None = None, adaptive: bool | None = None,
             max_steps: int = 1 << 40, residual_tol: float = 0.0, residual_every: int | None = None,
             convergence_threshold: float | None = None, check_frequency: int | None = None,
-            steps_per_graph: int = 0) -> RunResult:
+            steps_per_graph: int = 0, engine: str = "auto") -> RunResult:
         """Graph-resident driver loop (src/main.cpp:191-282).
 
         The L-inf residual (a separate pass over both state buffers) is
         evaluated every ``residual_every`` steps: by default every 50 steps
         when ``residual_tol`` is set, otherwise only for the final state.
+        ``engine``: "graph" (two kernels per step from captured CUDA graphs),
+        "persistent" (one cooperative launch for many steps; fast precision
+        without convergence_threshold) or "auto" (graph); both give the same bits.
         """
         cfg = self.cfg
         if residual_every is None:
@@ -119,6 +123,7 @@ class GpuSolver:
         p.residual_every = residual_every
         p.max_steps = int(max_steps)
         p.steps_per_graph = steps_per_graph
+        p.engine = ENGINES[engine]
         st = N.RunStats()
         rc = self.lib.mpd_run(self.h, C.byref(p), C.byref(st))
         if rc not in (N.MPD_OK, N.MPD_ERR_NONFINITE):

@@ -227,3 +227,44 @@ def test_bad_config_is_rejected_before_device_work(pkg):
         pkg.GpuSolver(cfg, case_geo, phys)
     assert ei.value.code == pkg._native.MPD_ERR_INVALID
     assert "AxisLF condition is only valid on the M_LO face" in str(ei.value)
+
+
+@pytest.mark.parametrize("name,cfg,steps,resid_every,T", [
+    ("channel_200x80", cases.channel_config(L=200, M=80), 700, 25, 1e300),
+    ("reference_default", cases.reference_default_config(L=80, M=40), 300, 7, 1e300),
+    ("edge_segments", cases.edge_config(), 200, 1, 1e300),
+    ("t_clamp", cases.channel_config(L=64, M=30, a=0.1), 100000, 10, 0.02),
+])
+def test_persistent_engine_matches_graph_engine(pkg, name, cfg, steps, resid_every, T):
+    """One cooperative launch per chunk of steps gives the graph path's bits:
+    the same state, t, dt, step count and residual schedule."""
+    case = cases.make_case(cfg)
+    res = {}
+    state = {}
+    for engine in ("graph", "persistent"):
+        solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+        r = solver.run(T=T, dt=cfg.dt, adaptive=True, max_steps=steps,
+                       residual_every=resid_every, engine=engine)
+        res[engine] = r
+        state[engine] = (solver.conserved(), solver.time(), solver.MaxWaveSpeed())
+        solver.close()
+    g, p = res["graph"], res["persistent"]
+    assert (p.steps, p.t, p.dt, p.max_wave_speed) == (g.steps, g.t, g.dt, g.max_wave_speed)
+    assert p.residual == g.residual
+    np.testing.assert_array_equal(state["persistent"][0], state["graph"][0])
+    assert state["persistent"][1:] == state["graph"][1:]
+
+
+def test_persistent_engine_stops_on_residual(pkg):
+    """residual_tol ends the persistent run at the same step as the graph run."""
+    cfg = cases.channel_config(L=40, M=16)
+    case = cases.make_case(cfg)
+    out = []
+    for engine in ("graph", "persistent"):
+        solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+        r = solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=200000, residual_tol=1e-5,
+                       residual_every=20, engine=engine)
+        out.append((r.steps, r.converged, r.residual, r.t))
+        solver.close()
+    assert out[0] == out[1]
+    assert out[0][1] and out[0][2] <= 1e-5
