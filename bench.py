@@ -179,7 +179,7 @@ def measured_hbm():
 
 def profiled_traffic():
     """DRAM bytes per interior-kernel launch from the committed ncu summary."""
-    p = ROOT / "profiles" / "lf_fast_kernel_1600x640.md"
+    p = ROOT / "profiles" / "lf_tma_kernel_1600x640.md"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
@@ -298,7 +298,7 @@ def run_ours(args, rank, world, local_rank):
             "config": workload_config(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
-                         "kernel": "lf_fast_kernel", "kernel_ms": int_ms,
+                         "kernel": "lf_tma_kernel", "kernel_ms": int_ms,
                          "bc_kernel_ms": bc_ms, "peak_source": hbm_src},
             "cpu_baseline": cpu,
             "e2e": {"value": world * CELLS * n_e2e / e2e_s, "unit": "cell-updates/s",
