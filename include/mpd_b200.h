@@ -227,6 +227,33 @@ int mpd_integrals_noalloc(const double *d_u, size_t plane_stride, int pitch, int
                           int M_max, const double *d_dr, double dz, double *d_out7,
                           void *stream);
 
+/* ---- batched solves: one persistent cooperative launch ------------------------ */
+/* New; the reference runs one solve per process.  A batch groups existing
+ * solvers (fast precision, one device) and runs them in one cooperative launch
+ * of persistent teams: team k is team_blocks[k] resident blocks (interior
+ * tasks of 30-column strips x row bands sized to the team, team-scoped
+ * barriers) and runs the solves with solve_team[i] == k one after the other,
+ * in increasing i.  Every solve takes exactly the steps, dt and residual
+ * schedule mpd_run would give it (same bits).  The plan (team sizes and the
+ * assignment) comes from the caller; the Python front end's autotuner times
+ * team sizes per grid shape and packs the solves. */
+typedef struct mpd_batch mpd_batch;
+
+/* The solvers stay owned by the caller and must outlive the batch. */
+int mpd_batch_create(mpd_solver *const *solvers, int n, mpd_batch **out);
+void mpd_batch_destroy(mpd_batch *b);
+/* Blocks one cooperative wave of the batch kernel holds on this device: the
+ * sum of team_blocks may not exceed it. */
+int mpd_batch_capacity(mpd_batch *b, int *blocks);
+/* Run every solve with the same run parameters (convergence_threshold must be
+ * 0; steps_per_graph = steps each solve may take per launch, 0 = 5000).
+ * stats: n entries.  solve_ms (n entries, or NULL): time from the first step
+ * any solve took in this run to this solve's last step.  device_ms (or NULL):
+ * the whole run. */
+int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *team_blocks,
+                  const int *solve_team, mpd_run_stats *stats, double *solve_ms,
+                  double *device_ms);
+
 /* ---- host-side expression initial condition ---------------------------------- */
 /* ExpressionIC::Apply, src/ics/expression_ic.cpp:286-324, evaluated on the host
  * with the library's expression compiler.  exprs: 8 strings in the

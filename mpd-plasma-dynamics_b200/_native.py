@@ -114,6 +114,11 @@ SIGNATURES = [
     ("mpd_profile_kernels", C.c_int, [_VP, C.c_int, C.c_double, DP]),
     ("mpd_integrals_noalloc", C.c_int, [_VP, C.c_size_t, C.c_int, C.c_int, C.c_int, _VP, C.c_double,
                                         _VP, _VP]),
+    ("mpd_batch_create", C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(_VP)]),
+    ("mpd_batch_destroy", None, [_VP]),
+    ("mpd_batch_capacity", C.c_int, [_VP, C.POINTER(C.c_int)]),
+    ("mpd_batch_run", C.c_int, [_VP, C.POINTER(RunParams), C.c_int, C.POINTER(C.c_int),
+                                C.POINTER(C.c_int), C.POINTER(RunStats), DP, DP]),
     ("mpd_expression_ic", C.c_int, [C.POINTER(Config), C.POINTER(Geometry), C.POINTER(C.c_char_p),
                                     C.c_int, C.POINTER(C.c_char_p), DP, DP]),
     ("mpd_eval_expression", C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), DP, DP]),

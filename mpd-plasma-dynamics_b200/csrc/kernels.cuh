@@ -29,6 +29,7 @@ struct DevState {
     unsigned int nf_acc, arrive;
     unsigned int res_nf, res_arrive;
     long long resid_step;
+    unsigned long long t0_ns, done_ns;  // persistent loops: first step taken, run done
 };
 
 constexpr int kFlagWs = 1;

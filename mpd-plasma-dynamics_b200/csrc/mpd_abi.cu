@@ -516,9 +516,8 @@ static int FinishRun(mpd_solver *s, long long step0, mpd_run_stats *stats) {
     return MPD_OK;
 }
 
-int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
-    int rc = CheckHandle(s);
-    if (rc != MPD_OK) return rc;
+// mpd_run's checks of the run parameters.
+static int CheckRunParams(const mpd_solver *s, const mpd_run_params *p) {
     if (!p) return Fail(MPD_ERR_INVALID, "run params are NULL");
     if (p->convergence_threshold > 0.0 && !s->with_prev)
         return Fail(MPD_ERR_INVALID, "convergence_threshold > 0 needs a solver created with with_prev");
@@ -527,12 +526,16 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
     if (p->max_steps <= 0) return Fail(MPD_ERR_INVALID, "max_steps must be positive");
     if (p->residual_every < 0 || p->residual_every > 4096)
         return Fail(MPD_ERR_INVALID, "residual_every must be in [0, 4096]");
-    const bool with_check = p->convergence_threshold > 0.0;
-    const bool want_ws = p->adaptive != 0;
-    rc = SyncState(s);
+    return MPD_OK;
+}
+
+// Put the device controller into run mode for `p` (the driver loop's state,
+// src/main.cpp:191-223, including the first T clamp).  step0 = step at entry.
+static int PrepareRun(mpd_solver *s, const mpd_run_params *p, long long &step0) {
+    int rc = SyncState(s);
     if (rc != MPD_OK) return rc;
     mpd::DevState &h = *s->h_st;
-    const long long step0 = h.step;
+    step0 = h.step;
     h.run_mode = 1;
     h.adaptive = p->adaptive ? 1 : 0;
     h.want_ws = p->adaptive ? 1 : 0;
@@ -550,12 +553,46 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
     h.done = 0;
     h.converged = 0;
     h.nonfinite = 0;
+    h.t0_ns = 0ull;
+    h.done_ns = 0ull;
     double dt = p->dt;
     if (h.t + dt > h.T) dt = h.T - h.t;  // src/main.cpp:221-223
     h.dt = dt;
     if (!(h.t < h.T)) h.done = 1;
-    rc = PushState(s);
+    return PushState(s);
+}
+
+// Arguments of the persistent loops for solver s, with a team of `blocks`.
+static mpd::PersistArgs PersistArgsOf(const mpd_solver *s, int nstrips, int nbands,
+                                      long long nsteps, long long resid_base) {
+    mpd::PersistArgs a{};
+    a.g = s->g;
+    a.buf0 = s->buf[0];
+    a.buf1 = s->buf[1];
+    a.cphys = s->cphys;
+    a.wall0 = s->wall[0];
+    a.wall1 = s->wall[1];
+    a.len = s->len;
+    a.bc = s->bc;
+    a.st = s->st;
+    a.nstrips = nstrips;
+    a.nbands = nbands;
+    a.nsteps = nsteps;
+    a.resid_base = resid_base;
+    return a;
+}
+
+int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
+    int rc = CheckHandle(s);
     if (rc != MPD_OK) return rc;
+    rc = CheckRunParams(s, p);
+    if (rc != MPD_OK) return rc;
+    const bool with_check = p->convergence_threshold > 0.0;
+    const bool want_ws = p->adaptive != 0;
+    long long step0 = 0;
+    rc = PrepareRun(s, p, step0);
+    if (rc != MPD_OK) return rc;
+    mpd::DevState &h = *s->h_st;
 
     MPD_CK(cudaEventRecord(s->ev0, s->stream));
     if (!h.done && s->host_step == 0) {
@@ -572,21 +609,9 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
     if (p->engine == MPD_ENGINE_PERSISTENT) {
         // one cooperative launch per chunk of steps; the residual keeps the
         // graph path's schedule: after steps (step - base) % residual_every == 0
-        mpd::PersistArgs a{};
-        a.g = s->g;
-        a.buf0 = s->buf[0];
-        a.buf1 = s->buf[1];
-        a.cphys = s->cphys;
-        a.wall0 = s->wall[0];
-        a.wall1 = s->wall[1];
-        a.len = s->len;
-        a.bc = s->bc;
-        a.st = s->st;
-        a.gs = s->gsync;
-        a.nstrips = s->pplan.nstrips;
-        a.nbands = s->pplan.nbands;
-        a.nsteps = 2000;
-        a.resid_base = step0 + ((!h.done && s->host_step == 0) ? 1 : 0);
+        const mpd::PersistArgs a =
+            PersistArgsOf(s, s->pplan.nstrips, s->pplan.nbands, 2000,
+                          step0 + ((!h.done && s->host_step == 0) ? 1 : 0));
         long long last = -1;
         for (;;) {
             MPD_CK(cudaMemcpyAsync(s->h_st, s->st, sizeof(mpd::DevState), cudaMemcpyDeviceToHost,
@@ -598,7 +623,8 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
             if (h.step == last) return Fail(MPD_ERR_TIMEOUT, "run loop made no progress");
             last = h.step;
             MPD_CK(cudaMemsetAsync(s->gsync, 0, sizeof(mpd::GridSync), s->stream));
-            MPD_CK(mpd::launch_lf_persist(s->pplan, s->tmap[0], s->tmap[1], a, s->stream));
+            MPD_CK(mpd::launch_lf_persist(s->pplan, s->tmap[0], s->tmap[1], a, s->gsync,
+                                          s->stream));
         }
         return FinishRun(s, step0, stats);
     }
@@ -884,6 +910,206 @@ int mpd_profile_kernels(mpd_solver *s, int steps, double dt, double out_ms[2]) {
 int mpd_device_bytes(mpd_solver *s, size_t *bytes) {
     if (!s || !bytes) return Fail(MPD_ERR_INVALID, "bad arguments");
     *bytes = s->dev_bytes;
+    return MPD_OK;
+}
+
+struct mpd_batch {
+    std::vector<mpd_solver *> solvers;
+    int device = 0;
+    int capacity = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    mpd::PersistArgs *d_solves = nullptr;
+    CUtensorMap *d_maps = nullptr;
+    int *d_ints = nullptr;            // team_first | solve_first | order
+    mpd::GridSync *d_gs = nullptr;    // one per team (at most one per solve)
+};
+
+static void FreeBatch(mpd_batch *b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    cudaFree(b->d_solves);
+    cudaFree(b->d_maps);
+    cudaFree(b->d_ints);
+    cudaFree(b->d_gs);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int mpd_batch_create(mpd_solver *const *solvers, int n, mpd_batch **out) {
+    if (!out) return Fail(MPD_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!solvers || n <= 0) return Fail(MPD_ERR_INVALID, "a batch needs at least one solver");
+    int dev = 0;
+    MPD_CK(cudaGetDevice(&dev));
+    for (int i = 0; i < n; ++i) {
+        const int rc = CheckHandle(solvers[i]);
+        if (rc != MPD_OK) return rc;
+        if (solvers[i]->precision != MPD_PRECISION_FAST || !solvers[i]->persist_ok)
+            return Fail(MPD_ERR_INVALID, "batched solvers must use MPD_PRECISION_FAST on a "
+                                         "device with cooperative launch");
+        if (solvers[i]->device != dev)
+            return Fail(MPD_ERR_INVALID, "batched solvers must live on the current device");
+    }
+    auto *b = new mpd_batch();
+    b->solvers.assign(solvers, solvers + n);
+    b->device = dev;
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        mpd::persist_blocks_per_sm(per_sm) != cudaSuccess || per_sm < 1) {
+        FreeBatch(b);
+        return Fail(MPD_ERR_CUDA, "occupancy query for the batch kernel failed");
+    }
+    b->capacity = sms * per_sm;
+    const size_t nints = 2 * (static_cast<size_t>(n) + 1) + n;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void **>(&b->d_solves), n * sizeof(mpd::PersistArgs)) !=
+            cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void **>(&b->d_maps), 2 * n * sizeof(CUtensorMap)) !=
+            cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void **>(&b->d_ints), nints * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void **>(&b->d_gs), n * sizeof(mpd::GridSync)) !=
+            cudaSuccess) {
+        FreeBatch(b);
+        return Fail(MPD_ERR_NOMEM, "batch allocation failed");
+    }
+    *out = b;
+    return MPD_OK;
+}
+
+void mpd_batch_destroy(mpd_batch *b) { FreeBatch(b); }
+
+int mpd_batch_capacity(mpd_batch *b, int *blocks) {
+    if (!b || !blocks) return Fail(MPD_ERR_INVALID, "NULL argument");
+    *blocks = b->capacity;
+    return MPD_OK;
+}
+
+int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *team_blocks,
+                  const int *solve_team, mpd_run_stats *stats, double *solve_ms,
+                  double *device_ms) {
+    if (!b) return Fail(MPD_ERR_INVALID, "batch handle is NULL");
+    const int n = static_cast<int>(b->solvers.size());
+    if (!team_blocks || !solve_team || nteams < 1 || nteams > n)
+        return Fail(MPD_ERR_INVALID, "bad team plan");
+    long long used = 0;
+    for (int k = 0; k < nteams; ++k) {
+        if (team_blocks[k] < 1) return Fail(MPD_ERR_INVALID, "a team needs at least one block");
+        used += team_blocks[k];
+    }
+    if (used > b->capacity)
+        return Fail(MPD_ERR_INVALID, "teams need " + std::to_string(used) + " blocks; one wave holds " +
+                                         std::to_string(b->capacity));
+    for (int i = 0; i < n; ++i)
+        if (solve_team[i] < 0 || solve_team[i] >= nteams)
+            return Fail(MPD_ERR_INVALID, "solve_team out of range");
+    if (p && p->convergence_threshold > 0.0)
+        return Fail(MPD_ERR_INVALID, "batched runs take no convergence_threshold");
+    const long long chunk = (p && p->steps_per_graph > 0) ? p->steps_per_graph : 5000;
+
+    // every solve: run mode, then the exact first step where the solve has none
+    std::vector<long long> step0(n), base(n);
+    for (int i = 0; i < n; ++i) {
+        mpd_solver *s = b->solvers[i];
+        int rc = CheckRunParams(s, p);
+        if (rc != MPD_OK) return rc;
+        rc = PrepareRun(s, p, step0[i]);
+        if (rc != MPD_OK) return rc;
+        MPD_CK(cudaEventRecord(s->ev0, s->stream));
+        const bool first = !s->h_st->done && s->host_step == 0;
+        if (first) {
+            rc = EnqueueStep(s, true, true, 0.0, false, p->adaptive != 0, p->residual_every == 1);
+            if (rc != MPD_OK) return rc;
+        }
+        base[i] = step0[i] + (first ? 1 : 0);
+    }
+    for (mpd_solver *s : b->solvers) MPD_CK(cudaStreamSynchronize(s->stream));
+
+    // plan: team block ranges, solves grouped by team, per-solve interior tasks
+    std::vector<int> team_first(nteams + 1, 0), solve_first(nteams + 1, 0), order;
+    for (int k = 0; k < nteams; ++k) team_first[k + 1] = team_first[k] + team_blocks[k];
+    for (int k = 0; k < nteams; ++k) {
+        solve_first[k] = static_cast<int>(order.size());
+        for (int i = 0; i < n; ++i)
+            if (solve_team[i] == k) order.push_back(i);
+    }
+    solve_first[nteams] = static_cast<int>(order.size());
+    std::vector<mpd::PersistArgs> args(n);
+    std::vector<CUtensorMap> maps(2 * n);
+    for (int i = 0; i < n; ++i) {
+        mpd_solver *s = b->solvers[i];
+        int nstrips = 0, nbands = 0;
+        mpd::persist_tasks(s->g, team_blocks[solve_team[i]], nstrips, nbands);
+        args[i] = PersistArgsOf(s, nstrips, nbands, chunk, base[i]);
+        maps[2 * i] = s->tmap[0];
+        maps[2 * i + 1] = s->tmap[1];
+    }
+    std::vector<int> ints;
+    ints.insert(ints.end(), team_first.begin(), team_first.end());
+    ints.insert(ints.end(), solve_first.begin(), solve_first.end());
+    ints.insert(ints.end(), order.begin(), order.end());
+    MPD_CK(cudaMemcpyAsync(b->d_solves, args.data(), n * sizeof(mpd::PersistArgs),
+                           cudaMemcpyHostToDevice, b->stream));
+    MPD_CK(cudaMemcpyAsync(b->d_maps, maps.data(), 2 * n * sizeof(CUtensorMap),
+                           cudaMemcpyHostToDevice, b->stream));
+    MPD_CK(cudaMemcpyAsync(b->d_ints, ints.data(), ints.size() * sizeof(int),
+                           cudaMemcpyHostToDevice, b->stream));
+    mpd::BatchArgs ba{};
+    ba.solves = b->d_solves;
+    ba.maps = b->d_maps;
+    ba.team_first = b->d_ints;
+    ba.solve_first = b->d_ints + (nteams + 1);
+    ba.order = b->d_ints + 2 * (nteams + 1);
+    ba.gs = b->d_gs;
+    ba.nteams = nteams;
+    const int blocks = team_first[nteams];
+
+    MPD_CK(cudaEventRecord(b->ev0, b->stream));
+    long long last = -1;
+    for (;;) {
+        MPD_CK(cudaMemsetAsync(b->d_gs, 0, nteams * sizeof(mpd::GridSync), b->stream));
+        MPD_CK(mpd::launch_lf_batch(blocks, ba, b->stream));
+        long long total = 0;
+        bool all_done = true, failed = false;
+        for (mpd_solver *s : b->solvers)
+            MPD_CK(cudaMemcpyAsync(s->h_st, s->st, sizeof(mpd::DevState), cudaMemcpyDeviceToHost,
+                                   b->stream));
+        MPD_CK(cudaStreamSynchronize(b->stream));
+        for (mpd_solver *s : b->solvers) {
+            total += s->h_st->step;
+            all_done = all_done && s->h_st->done;
+            failed = failed || s->h_st->wait_fail;
+        }
+        if (failed)
+            return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
+        if (all_done) break;
+        if (total == last) return Fail(MPD_ERR_TIMEOUT, "batch run made no progress");
+        last = total;
+    }
+    MPD_CK(cudaEventRecord(b->ev1, b->stream));
+    MPD_CK(cudaEventSynchronize(b->ev1));
+    float ms = 0.f;
+    MPD_CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    if (device_ms) *device_ms = ms;
+    unsigned long long t_first = ~0ull;
+    std::vector<unsigned long long> done_ns(n);
+    for (int i = 0; i < n; ++i) {
+        const mpd::DevState &h = *b->solvers[i]->h_st;
+        if (h.t0_ns && h.t0_ns < t_first) t_first = h.t0_ns;
+        done_ns[i] = h.done_ns;
+    }
+    int status = MPD_OK;
+    for (int i = 0; i < n; ++i) {
+        if (solve_ms)
+            solve_ms[i] = (done_ns[i] && t_first != ~0ull) ? (done_ns[i] - t_first) * 1e-6 : NAN;
+        const int rc = FinishRun(b->solvers[i], step0[i], stats ? &stats[i] : nullptr);
+        if (rc == MPD_ERR_NONFINITE) status = rc;
+        else if (rc != MPD_OK) return rc;
+    }
+    if (status != MPD_OK) return Fail(status, "non-finite value in a batched solve");
     return MPD_OK;
 }
 

@@ -48,31 +48,10 @@ def make_case(cfg) -> Case:
 
 def channel_config(L=200, M=80, a=0.0, beta=0.1, amp=1.0, vz=0.1, gamma=5.0 / 3.0,
                    adaptive=True, cfl=0.4) -> object:
-    """The straight / sine-wall coaxial channel of the plain-method workloads.
-
-    r1 = 0.2, r2(z) = 0.8 - a sin(pi z); IC rho = 1, v_z = vz, v_r = v_phi = 0,
-    p = beta/2, B_phi = amp r1 / r, B_z = B_r = 0; inlet fixed at the IC
-    values, zero-gradient outlet, slip walls.
-    """
-    cfg = SimConfig(gamma=gamma, beta=beta, H_z0=0.0, L_max=L, M_max=M,
-                    adaptive_dt=adaptive, cfl_number=cfl, dt_growth_factor=1.1,
-                    dt_min=1e-12, dt_max=1.0, dt=1e-5, T=1e300)
-    cfg.geometry = pkg.config.GeometryConfig("sine_wall", {"r1": 0.2, "r2": 0.8, "a": a})
-    hphi = "0.2 / r" if amp == 1.0 else f"{amp!r} * 0.2 / r"
-    e_expr = "beta / (2 * (gamma - 1))"
-    cfg.initial_conditions = pkg.config.ICConfig(params={
-        "rho": "1", "v_z": repr(vz), "v_r": "0", "v_phi": "0", "H_z": "0", "H_r": "0",
-        "H_phi": hphi, "e": e_expr})
-    cfg.bc_l_lo.segments = [segment(rho=("dirichlet", 1.0), v_z=("dirichlet", vz),
-                                    v_r=("dirichlet", 0.0), v_phi=("dirichlet", 0.0),
-                                    H_z=("dirichlet", 0.0), H_r=("dirichlet", 0.0),
-                                    e=("expr", e_expr), H_phi=("expr", hphi))]
-    cfg.bc_l_hi.segments = [segment()]
-    wall = dict(v_r=("expr", "v_z * r_z"), H_r=("expr", "H_z * r_z"))
-    cfg.bc_m_lo.segments = [segment(**wall)]
-    cfg.bc_m_hi.segments = [segment(**wall)]
-    cfg.init()
-    return cfg
+    """The straight / sine-wall coaxial channel of the plain-method workloads
+    (mpd_b200.workloads.channel_config)."""
+    return pkg.workloads.channel_config(L=L, M=M, a=a, beta=beta, amp=amp, vz=vz, gamma=gamma,
+                                        adaptive=adaptive, cfl=cfl)
 
 
 def channel_case(**kw) -> Case:
