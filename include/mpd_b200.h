@@ -254,6 +254,29 @@ int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *
                   const int *solve_team, mpd_run_stats *stats, double *solve_ms,
                   double *device_ms);
 
+/* ---- surrogate network kernels (learned warm start) -------------------------- */
+/* New; the reference has no learned component.  Device pointers, FP32 in
+ * global memory; the GEMM rounds its operands to BF16 and accumulates in FP32
+ * on the tcgen05 tensor cores:
+ *   C[b](m,n) = alpha * sum_k A[b](m,k) B[b](n,k) + beta * C[b](m,n)
+ * with element strides per operand (row, k, batch) so transposed operands
+ * need no copy.  beta == 0 never reads C.  Launches on `stream` and returns
+ * at once; mpd_nn_wait_status synchronises the stream and reports a tensor-
+ * core wait that gave up (MPD_ERR_TIMEOUT). */
+typedef struct mpd_gemm_desc {
+    int M, N, K, batch;
+    const float *A;
+    long long sam, sak, sab;
+    const float *B;
+    long long sbn, sbk, sbb;
+    float *C;
+    long long scm, scn, scb;
+    float alpha, beta;
+} mpd_gemm_desc;
+
+int mpd_nn_gemm(const mpd_gemm_desc *d, void *stream);
+int mpd_nn_wait_status(void *stream);
+
 /* ---- host-side expression initial condition ---------------------------------- */
 /* ExpressionIC::Apply, src/ics/expression_ic.cpp:286-324, evaluated on the host
  * with the library's expression compiler.  exprs: 8 strings in the

@@ -78,6 +78,17 @@ class RunStats(C.Structure):
                 ("device_ms", C.c_double)]
 
 
+class GemmDesc(C.Structure):
+    _fields_ = [("M", C.c_int), ("N", C.c_int), ("K", C.c_int), ("batch", C.c_int),
+                ("A", C.c_void_p), ("sam", C.c_longlong), ("sak", C.c_longlong),
+                ("sab", C.c_longlong),
+                ("B", C.c_void_p), ("sbn", C.c_longlong), ("sbk", C.c_longlong),
+                ("sbb", C.c_longlong),
+                ("C", C.c_void_p), ("scm", C.c_longlong), ("scn", C.c_longlong),
+                ("scb", C.c_longlong),
+                ("alpha", C.c_float), ("beta", C.c_float)]
+
+
 class MpdError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
@@ -119,6 +130,8 @@ SIGNATURES = [
     ("mpd_batch_capacity", C.c_int, [_VP, C.POINTER(C.c_int)]),
     ("mpd_batch_run", C.c_int, [_VP, C.POINTER(RunParams), C.c_int, C.POINTER(C.c_int),
                                 C.POINTER(C.c_int), C.POINTER(RunStats), DP, DP]),
+    ("mpd_nn_gemm", C.c_int, [C.POINTER(GemmDesc), _VP]),
+    ("mpd_nn_wait_status", C.c_int, [_VP]),
     ("mpd_expression_ic", C.c_int, [C.POINTER(Config), C.POINTER(Geometry), C.POINTER(C.c_char_p),
                                     C.c_int, C.POINTER(C.c_char_p), DP, DP]),
     ("mpd_eval_expression", C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), DP, DP]),
