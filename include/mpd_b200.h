@@ -277,6 +277,23 @@ typedef struct mpd_gemm_desc {
 int mpd_nn_gemm(const mpd_gemm_desc *d, void *stream);
 int mpd_nn_wait_status(void *stream);
 
+/* Element-wise and reduction kernels of the network (FP32, deterministic sums):
+ * z += bias (per column), out = GELU(z) (act != 0) or z;  g_z = g_out GELU'(z);
+ * out[c] = sum over rows of x[r][c];  out (+)= sum of nparts arrays of n;
+ * mean squared error of pred vs target into *loss (one double) with
+ * grad = 2 (pred - target) / n (grad may be NULL), partial = scratch of
+ * 148 * 32 doubles;  one Adam step (bias-corrected, step >= 1). */
+int mpd_nn_bias_act(float *z, const float *bias, float *out, long long rows, int cols, int act,
+                    void *stream);
+int mpd_nn_act_bwd(const float *g_out, const float *z, float *g_z, long long n, void *stream);
+int mpd_nn_colsum(const float *x, long long rows, int cols, float *out, void *stream);
+int mpd_nn_sum_parts(const float *parts, int nparts, long long n, float *out, int accumulate,
+                     void *stream);
+int mpd_nn_mse(const float *pred, const float *target, long long n, float *grad, double *partial,
+               double *loss, void *stream);
+int mpd_nn_adam(float *p, const float *g, float *m, float *v, long long n, float lr, float b1,
+                float b2, float eps, int step, void *stream);
+
 /* ---- host-side expression initial condition ---------------------------------- */
 /* ExpressionIC::Apply, src/ics/expression_ic.cpp:286-324, evaluated on the host
  * with the library's expression compiler.  exprs: 8 strings in the

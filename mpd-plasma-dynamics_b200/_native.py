@@ -132,6 +132,13 @@ SIGNATURES = [
                                 C.POINTER(C.c_int), C.POINTER(RunStats), DP, DP]),
     ("mpd_nn_gemm", C.c_int, [C.POINTER(GemmDesc), _VP]),
     ("mpd_nn_wait_status", C.c_int, [_VP]),
+    ("mpd_nn_bias_act", C.c_int, [_VP, _VP, _VP, C.c_longlong, C.c_int, C.c_int, _VP]),
+    ("mpd_nn_act_bwd", C.c_int, [_VP, _VP, _VP, C.c_longlong, _VP]),
+    ("mpd_nn_colsum", C.c_int, [_VP, C.c_longlong, C.c_int, _VP, _VP]),
+    ("mpd_nn_sum_parts", C.c_int, [_VP, C.c_int, C.c_longlong, _VP, C.c_int, _VP]),
+    ("mpd_nn_mse", C.c_int, [_VP, _VP, C.c_longlong, _VP, _VP, _VP, _VP]),
+    ("mpd_nn_adam", C.c_int, [_VP, _VP, _VP, _VP, C.c_longlong, C.c_float, C.c_float, C.c_float,
+                              C.c_float, C.c_int, _VP]),
     ("mpd_expression_ic", C.c_int, [C.POINTER(Config), C.POINTER(Geometry), C.POINTER(C.c_char_p),
                                     C.c_int, C.POINTER(C.c_char_p), DP, DP]),
     ("mpd_eval_expression", C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), DP, DP]),

@@ -1,0 +1,62 @@
+"""The surrogate network on the GPU (tcgen05 BF16 GEMMs, FP32 element-wise
+kernels) against its CPU oracle with the same BF16 operand rounding:
+forward output, loss and every parameter gradient; and Adam training that
+lowers the loss."""
+import numpy as np
+import pytest
+
+import __graft_entry__
+from oracle import surrogate_oracle as so
+
+pytestmark = pytest.mark.gpu
+pkg = __graft_entry__.load_package()
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def setup(H=12, W=9, B=2, seed=0):
+    import torch
+    rng = np.random.default_rng(seed)
+    params = pkg.surrogate.init_params(seed=seed + 1)
+    x = rng.standard_normal((B, H * W, so.N_IN))
+    target = rng.standard_normal((B, H * W, so.N_OUT))
+    net = pkg.surrogate.SpectralOperator(H, W, B, params=params)
+    net.load_inputs(x)
+    tgt = torch.from_numpy(target.reshape(-1, so.N_OUT).astype(np.float32)).cuda()
+    return params, x, target, net, tgt
+
+
+def test_forward_and_gradients_match_oracle():
+    params, x, target, net, tgt = setup()
+    out = net.forward()
+    net.loss_and_grad(tgt)
+    net.backward()
+    net.wait()
+    ora = so.Oracle(12, 9, bf16=True)
+    # the oracle sees the parameters as the GPU holds them (FP32)
+    p32 = {k: v.astype(np.float32).astype(np.float64) for k, v in params.items()}
+    x32 = x.astype(np.float32).astype(np.float64)
+    t32 = target.astype(np.float32).astype(np.float64)
+    o_out, saved = ora.forward(p32, x32)
+    got = out.cpu().numpy().reshape(o_out.shape)
+    assert rel(got, o_out) < 1e-2
+    assert abs(float(net.loss.cpu()[0]) - ora.loss(got, t32)) <= 1e-6 * ora.loss(got, t32)
+    o_g = ora.backward(p32, saved, o_out, t32)
+    g = net.grads()
+    for k in o_g:
+        assert rel(g[k], o_g[k]) < 3e-2, (k, rel(g[k], o_g[k]))
+
+
+def test_adam_training_lowers_the_loss():
+    params, x, target, net, tgt = setup(H=10, W=8, B=2, seed=4)
+    losses = []
+    for _ in range(60):
+        net.forward()
+        net.loss_and_grad(tgt)
+        net.backward()
+        net.adam_step(lr=2e-3)
+        losses.append(float(net.loss.cpu()[0]))
+    net.wait()
+    assert losses[-1] < 0.5 * losses[0], losses[::10]
