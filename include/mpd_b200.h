@@ -125,7 +125,8 @@ int mpd_advance(mpd_solver *s, double dt);
 
 typedef struct mpd_run_params {
     double T;                   /* end time (use a huge value for step-limited runs) */
-    double dt;                  /* initial dt (SimConfig::dt)                         */
+    double dt;                  /* initial dt (SimConfig::dt); <= 0: the CFL limit of
+                                   the current state (warm starts)                    */
     int adaptive;               /* SimConfig::adaptive_dt                             */
     double cfl_number, dt_growth_factor, dt_min, dt_max;
     double convergence_threshold; /* relative-L2 change threshold, 0 = off          */

@@ -532,6 +532,13 @@ static int CheckRunParams(const mpd_solver *s, const mpd_run_params *p) {
 // Put the device controller into run mode for `p` (the driver loop's state,
 // src/main.cpp:191-223, including the first T clamp).  step0 = step at entry.
 static int PrepareRun(mpd_solver *s, const mpd_run_params *p, long long &step0) {
+    // dt <= 0: start at the CFL limit of the current state (a warm start that
+    // begins at the step the steady state was converged with)
+    double ws0 = 0.0;
+    if (!(p->dt > 0.0)) {
+        const int rw = mpd_max_wave_speed(s, &ws0);
+        if (rw != MPD_OK) return rw;
+    }
     int rc = SyncState(s);
     if (rc != MPD_OK) return rc;
     mpd::DevState &h = *s->h_st;
@@ -556,6 +563,11 @@ static int PrepareRun(mpd_solver *s, const mpd_run_params *p, long long &step0) 
     h.t0_ns = 0ull;
     h.done_ns = 0ull;
     double dt = p->dt;
+    if (!(dt > 0.0)) {
+        const double dx = s->g.dy < s->g.dz ? s->g.dy : s->g.dz;
+        dt = p->cfl_number * dx / (ws0 + 1.0e-10);
+        dt = dt < p->dt_min ? p->dt_min : (dt > p->dt_max ? p->dt_max : dt);
+    }
     if (h.t + dt > h.T) dt = h.T - h.t;  // src/main.cpp:221-223
     h.dt = dt;
     if (!(h.t < h.T)) h.done = 1;

@@ -91,19 +91,27 @@ def init_params(seed: int = 0, **kw) -> dict[str, np.ndarray]:
 
 @dataclasses.dataclass
 class Normalizer:
+    """Per-field affine normalisation of the targets.  A field that is the
+    same constant in every training state (v_phi, H_z, H_r of the channel
+    are identically zero) is not learned: decode returns the constant
+    exactly, so a warm start keeps it exact (the per-field relative residual
+    would otherwise see the network's tiny output there as a large change)."""
     mean: np.ndarray   # per field
     std: np.ndarray
+    const: np.ndarray  # per field: True if constant in the training data
 
     @classmethod
     def fit(cls, fields: np.ndarray) -> "Normalizer":
         f = fields.reshape(-1, N_OUT)
-        return cls(f.mean(0), np.maximum(f.std(0), 1e-6))
+        mean, std = f.mean(0), f.std(0)
+        const = std <= 1e-12 * np.maximum(1.0, np.abs(mean))
+        return cls(mean, np.where(const, 1.0, std), const)
 
     def encode(self, f):
-        return (f - self.mean) / self.std
+        return np.where(self.const, 0.0, (f - self.mean) / self.std)
 
     def decode(self, f):
-        return f * self.std + self.mean
+        return np.where(self.const, self.mean, f * self.std + self.mean)
 
 
 class SpectralOperator:

@@ -1,0 +1,278 @@
+"""Learned warm start of steady-state solves: data generation with the batched
+solver, surrogate training on the GPU, and the warm-versus-cold comparison.
+
+Pipeline:
+  1. steady states of the channel for parameter draws of the sweep box
+     (workloads.sweep_params on one grid), solved by BatchSolver until the
+     L-inf residual is <= tol (max max_steps steps);
+  2. the spectral operator (surrogate.SpectralOperator) trained on them:
+     inputs = parameters + (r, z), targets = the 8 primitive fields
+     normalised per field, Adam, mean squared error;
+  3. held-out draws solved twice by BatchSolver: from the initial condition
+     of the workload (cold) and from the surrogate's prediction (warm);
+     steps to converge, solves per second and the surrogate's own L-inf error
+     against the converged state are reported.  The plain time march stays
+     the judge: a warm solve is accepted only at residual <= tol, and a
+     prediction that fails (non-finite, non-positive density or energy) falls
+     back to the cold initial condition.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import time
+
+import numpy as np
+
+from . import surrogate as S
+from .batch import Autotuner, BatchPlan, BatchSolver
+from .geometry import GeometryRegistry, Grid
+from .ic import ArrayIC, derived_pressures
+from .solver import GpuSolver, build_case
+from .workloads import SweepParams, sweep_params
+
+# physical plane index of each network field (rho, v_z, v_r, v_phi, e, H_z, H_r, H_phi)
+PLANE_OF_FIELD = (0, 1, 2, 3, 4, 7, 8, 9)
+
+
+def draws(seeds, grid):
+    return [sweep_params(int(s), grids=(grid,)) for s in seeds]
+
+
+def grid_of(cfg) -> Grid:
+    geom = GeometryRegistry.Instance().Create(cfg.geometry.type, cfg.geometry.params)
+    return Grid(cfg, geom)
+
+
+def inputs_of(p: SweepParams, grid: Grid) -> np.ndarray:
+    cfg = grid.cfg
+    L, M = cfg.L_max, cfg.M_max
+    r = grid.r[1:L + 1, 1:M + 2]
+    z = (np.arange(1, L + 1) - 1) * cfg.dz
+    return S.features(S.param_vector(p.amp, p.beta, p.vz, p.a), r, z)
+
+
+def fields_of(phys10: np.ndarray, L: int, M: int) -> np.ndarray:
+    """H x W x 8 network fields from the 10 physical planes."""
+    return np.stack([phys10[k, 1:L + 1, 1:M + 2] for k in PLANE_OF_FIELD], axis=-1)
+
+
+def planes_from_fields(f: np.ndarray, cfg, floor: np.ndarray) -> np.ndarray:
+    """10 physical planes from H x W x 8 predicted fields (density and energy
+    kept above `floor`), p and P derived as ExpressionIC derives them."""
+    L, M = cfg.L_max, cfg.M_max
+    phys = np.zeros((10, L + 2, M + 3))
+    for j, k in enumerate(PLANE_OF_FIELD):
+        phys[k, 1:L + 1, 1:M + 2] = f[..., j]
+    phys[0] = np.maximum(phys[0], floor[0])
+    phys[4] = np.maximum(phys[4], floor[1])
+    derived_pressures(phys, cfg.gamma)
+    return phys
+
+
+@dataclasses.dataclass
+class SolveSet:
+    steps: np.ndarray
+    converged: np.ndarray
+    residual: np.ndarray
+    fields: list            # H x W x 8 per solve (final state)
+    device_ms: float        # sum over the batch launches
+    solve_ms: np.ndarray
+
+
+def solve_all(params: list[SweepParams], ics: list | None = None, max_steps=200_000, tol=1e-8,
+              every=50, chunk: int = 256, tuner: Autotuner | None = None) -> SolveSet:
+    """Solve every draw with the batched engine, in batches of at most `chunk`
+    solves, from the workload's initial condition (the workload's dt0) or,
+    with ics, from the given planes starting at their CFL dt: the LF steady
+    state depends on dt, so a warm start that ramps dt up from dt0 would
+    leave the steady state it was given."""
+    n = len(params)
+    steps = np.zeros(n, dtype=np.int64)
+    conv = np.zeros(n, dtype=bool)
+    res = np.full(n, np.nan)
+    fields = [None] * n
+    solve_ms = np.zeros(n)
+    dev_ms = 0.0
+    for i0 in range(0, n, chunk):
+        part = params[i0:i0 + chunk]
+        cfgs = [p.config() for p in part]
+        solvers = []
+        for k, cfg in enumerate(cfgs):
+            ic = ics[i0 + k] if ics is not None else None
+            if ic is None:
+                solvers.append(build_case(cfg, precision="fast"))
+            else:
+                solvers.append(GpuSolver(cfg, grid_of(cfg), ic, precision="fast"))
+        batch = BatchSolver(solvers)
+        tuner = tuner or Autotuner(batch.capacity, steps=100)
+        plan = tuner.plan(cfgs, max_steps=max_steps)
+        out = batch.run(plan, dt=None if ics is None else 0.0, max_steps=max_steps,
+                        residual_tol=tol, residual_every=every)
+        dev_ms += out.device_ms
+        for k, (s, r) in enumerate(zip(solvers, out.runs)):
+            j = i0 + k
+            steps[j], conv[j], res[j] = r.steps, r.converged, r.residual
+            solve_ms[j] = out.solve_ms[k]
+            fields[j] = fields_of(s.physical(), s.cfg.L_max, s.cfg.M_max)
+        batch.close()
+        for s in solvers:
+            s.close()
+    return SolveSet(steps, conv, res, fields, dev_ms, solve_ms)
+
+
+@dataclasses.dataclass
+class Trained:
+    net: S.SpectralOperator
+    norm: S.Normalizer
+    losses: list
+    train_s: float
+
+
+def train(X: np.ndarray, Y: np.ndarray, H: int, W: int, epochs: int = 40, batch: int = 16,
+          lr: float = 1e-3, seed: int = 0, log=None) -> Trained:
+    """X: N x P x 6 inputs, Y: N x P x 8 fields (physical units)."""
+    import torch
+    norm = S.Normalizer.fit(Y)
+    Yn = norm.encode(Y).astype(np.float32)
+    dev = torch.device("cuda")
+    dX = torch.from_numpy(X.astype(np.float32)).to(dev)
+    dY = torch.from_numpy(Yn).to(dev)
+    net = S.SpectralOperator(H, W, batch, seed=seed)
+    rng = np.random.default_rng(seed)
+    N = len(X)
+    nb = N // batch
+    losses = []
+    t0 = time.perf_counter()
+    total = epochs * nb
+    it = 0
+    for ep in range(epochs):
+        perm = torch.from_numpy(rng.permutation(N)[:nb * batch]).to(dev)
+        ep_loss = 0.0
+        for b in range(nb):
+            idx = perm[b * batch:(b + 1) * batch]
+            net.x.copy_(dX.index_select(0, idx).reshape(-1, S.N_IN))
+            tgt = dY.index_select(0, idx).reshape(-1, S.N_OUT)
+            net.forward()
+            net.loss_and_grad(tgt)
+            net.backward()
+            rate = lr * 0.5 * (1 + math.cos(math.pi * it / total)) + 1e-5
+            net.adam_step(lr=rate)
+            ep_loss += float(net.loss.cpu()[0]) if b == nb - 1 else 0.0
+            it += 1
+        losses.append(ep_loss)
+        if log:
+            log(f"epoch {ep} loss {ep_loss:.4e}")
+    net.wait()
+    return Trained(net, norm, losses, time.perf_counter() - t0)
+
+
+def predict(tr: Trained, X: np.ndarray) -> tuple[np.ndarray, float]:
+    """N x P x 8 fields (physical units) and the device seconds it took."""
+    import torch
+    net = tr.net
+    B = net.B
+    N = len(X)
+    out = np.zeros((N, X.shape[1], S.N_OUT))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(0, N, B):
+        xb = np.zeros((B,) + X.shape[1:], dtype=np.float32)
+        k = min(B, N - i)
+        xb[:k] = X[i:i + k]
+        net.load_inputs(xb)
+        y = net.forward()
+        out[i:i + k] = y.cpu().numpy().reshape(B, X.shape[1], S.N_OUT)[:k]
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    return tr.norm.decode(out), dt
+
+
+def relative_linf(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Per field max |a - b| / max |b|."""
+    return np.abs(a - b).reshape(-1, S.N_OUT).max(0) / np.maximum(
+        np.abs(b).reshape(-1, S.N_OUT).max(0), 1e-30)
+
+
+def run_pipeline(n_train=2000, n_eval=256, grid=(100, 40), epochs=40, batch=16, lr=1e-3,
+                 max_steps=200_000, tol=1e-8, plain_sample=4, log=print) -> dict:
+    """Steps 1-3 of the module docstring; returns the measurements."""
+    L, M = grid
+    H, W = L, M + 1
+    train_p = draws(range(n_train), grid)
+    eval_p = draws(range(1_000_000, 1_000_000 + n_eval), grid)
+    tuner = None
+    t0 = time.perf_counter()
+    data = solve_all(train_p, max_steps=max_steps, tol=tol)
+    gen_s = time.perf_counter() - t0
+    keep = np.flatnonzero(data.converged)
+    log(f"training solves: {len(keep)} of {n_train} converged, {gen_s:.1f} s")
+    grids = [grid_of(p.config()) for p in train_p[:1]]
+    X = np.stack([inputs_of(train_p[i], grids[0]) for i in keep])
+    Y = np.stack([data.fields[i].reshape(H * W, S.N_OUT) for i in keep])
+    tr = train(X, Y, H, W, epochs=epochs, batch=batch, lr=lr, log=log)
+    log(f"trained {epochs} epochs in {tr.train_s:.1f} s, final loss {tr.losses[-1]:.3e}")
+
+    Xe = np.stack([inputs_of(p, grids[0]) for p in eval_p])
+    pred, infer_s = predict(tr, Xe)
+    floor = np.array([0.05 * np.min(Y[..., 0]), 0.05 * np.min(Y[..., 4])])
+    cfg0 = eval_p[0].config()
+    ics = []
+    fallback = 0
+    for p, f in zip(eval_p, pred):
+        f = f.reshape(H, W, S.N_OUT)
+        if not np.all(np.isfinite(f)):
+            ics.append(None)
+            fallback += 1
+            continue
+        ics.append(planes_from_fields(f, p.config(), floor))
+    cold = solve_all(eval_p, max_steps=max_steps, tol=tol)
+    warm = solve_all(eval_p, ics=ics, max_steps=max_steps, tol=tol)
+    both = cold.converged & warm.converged
+    log(f"eval: cold converged {int(cold.converged.sum())}, warm converged "
+        f"{int(warm.converged.sum())} of {n_eval}; steps cold median "
+        f"{np.median(cold.steps):.0f}, warm median {np.median(warm.steps):.0f}; warm residuals "
+        f"{np.nanmedian(warm.residual):.2e}")
+    err = [relative_linf(pred[i].reshape(H, W, S.N_OUT), cold.fields[i])
+           for i in np.flatnonzero(cold.converged)]
+    err = np.stack(err) if err else np.full((1, S.N_OUT), np.nan)
+    agree = [relative_linf(warm.fields[i], cold.fields[i]) for i in np.flatnonzero(both)]
+    agree = np.stack(agree) if agree else None
+
+    # the plain FP64 time march, one solve after another (graph engine)
+    seq_ms, seq_steps = 0.0, 0
+    for p in eval_p[:plain_sample]:
+        s = build_case(p.config(), precision="fast")
+        r = s.run(T=1e300, dt=cfg0.dt, adaptive=True, max_steps=max_steps, residual_tol=tol,
+                  residual_every=50, engine="graph")
+        seq_ms += r.device_ms
+        seq_steps += r.steps
+        s.close()
+    plain_sps = plain_sample / (seq_ms * 1e-3)
+    cold_sps = n_eval / (cold.device_ms * 1e-3)
+    warm_sps = n_eval / (warm.device_ms * 1e-3 + infer_s)
+    return {
+        "grid": f"{L}x{M}", "n_train": n_train, "n_train_converged": int(len(keep)),
+        "n_eval": n_eval, "epochs": epochs, "data_gen_s": gen_s, "train_s": tr.train_s,
+        "final_loss": tr.losses[-1], "losses": tr.losses,
+        "cold_converged": int(cold.converged.sum()), "warm_converged": int(warm.converged.sum()),
+        "warm_fallback_to_cold_ic": fallback,
+        "cold_steps_mean": float(cold.steps.mean()), "warm_steps_mean": float(warm.steps.mean()),
+        "cold_steps_median": float(np.median(cold.steps)),
+        "warm_steps_median": float(np.median(warm.steps)),
+        "cold_batch_solves_per_s": cold_sps, "warm_batch_solves_per_s": warm_sps,
+        "plain_sequential_solves_per_s": plain_sps,
+        "plain_sequential_sample": plain_sample,
+        "warm_over_plain": warm_sps / plain_sps, "warm_over_cold_batch": warm_sps / cold_sps,
+        "surrogate_inference_s": infer_s,
+        "surrogate_rel_linf_median": np.median(err, 0).tolist(),
+        "surrogate_rel_linf_max": err.max(0).tolist(),
+        "warm_vs_cold_state_rel_linf_max": agree.max(0).tolist() if agree is not None else None,
+        "both_converged": int(both.sum()),
+        "cold_steps_both": float(cold.steps[both].mean()) if both.any() else None,
+        "warm_steps_both": float(warm.steps[both].mean()) if both.any() else None,
+        "warm_p50_ms": float(np.percentile(warm.solve_ms, 50)),
+        "warm_p99_ms": float(np.percentile(warm.solve_ms, 99)),
+        "cold_p50_ms": float(np.percentile(cold.solve_ms, 50)),
+        "cold_p99_ms": float(np.percentile(cold.solve_ms, 99)),
+    }
