@@ -46,6 +46,16 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="lean run for ncu: warm-up, then --steps eager time steps, no extras")
     ap.add_argument("--precision", choices=("fast", "exact"), default="fast")
+    ap.add_argument("--workload", choices=("plain", "warmstart", "batch"), default="plain",
+                    help="plain: the 1600x640 time step (default); warmstart: surrogate-warm-"
+                         "started batched steady solves vs the plain time march; batch: the "
+                         "batched sweep of uneven grids")
+    ap.add_argument("--n-train", type=int, default=2000)
+    ap.add_argument("--n-eval", type=int, default=256)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--grid", type=str, default="100x40")
+    ap.add_argument("--n-solves", type=int, default=64)
+    ap.add_argument("--max-steps", type=int, default=200000)
     return ap.parse_args()
 
 
@@ -312,6 +322,66 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+def run_warmstart(args):
+    """Learned warm start (the sweep box on one grid): steady states from the
+    batched solver train the surrogate; held-out draws are then solved cold
+    and warm by the batched solver, and a sample of them one after another by
+    the plain FP64 time march (graph engine).  value = warm-start batch
+    solves/s (surrogate inference included)."""
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    L, M = (int(v) for v in args.grid.split("x"))
+    res = pkg.warmstart.run_pipeline(n_train=args.n_train, n_eval=args.n_eval, grid=(L, M),
+                                     epochs=args.epochs, max_steps=args.max_steps,
+                                     log=lambda m: print(m, file=sys.stderr, flush=True))
+    losses = res.pop("losses")
+    return {
+        "metric": "steady solves/s, warm-start batch (residual <= 1e-8)",
+        "value": res["warm_batch_solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+        "higher_is_better": True, "dtype": "f64 solver, bf16/f32 surrogate",
+        "data": "synthetic (sweep-box draws, numpy default_rng(seed))",
+        "config": {"workload": f"learned warm start, channel sweep box on {L}x{M}",
+                   "n_train": args.n_train, "n_eval": args.n_eval, "epochs": args.epochs,
+                   "surrogate": "4 spectral layers, 64 channels, 8 modes per axis"},
+        "vs_baseline": None, "loss_first_last": [losses[0], losses[-1]], **res}
+
+
+def run_batch(args):
+    """The batched sweep: n solves drawn from the sweep box (uneven grids),
+    autotuned teams, one persistent cooperative launch, cold start."""
+    import numpy as np
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    params = [pkg.workloads.sweep_params(i) for i in range(args.n_solves)]
+    cfgs = [p.config() for p in params]
+    solvers = [pkg.build_case(c, precision="fast") for c in cfgs]
+    batch = pkg.BatchSolver(solvers)
+    tuner = pkg.Autotuner(batch.capacity, steps=100)
+    plan = tuner.plan(cfgs, max_steps=args.max_steps)
+    res = batch.run(plan, max_steps=args.max_steps, residual_tol=1e-8, residual_every=50)
+    cells = sum(c.L_max * (c.M_max + 1) * r.steps for c, r in zip(cfgs, res.runs))
+    line = {
+        "metric": "batched steady solves: solves/s", "unit": "solves/s", "n_gpus": 1,
+        "value": args.n_solves / (res.device_ms * 1e-3), "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic (sweep-box draws, numpy default_rng(i))",
+        "config": {"workload": "batched sweep, grids {100x40,200x80,400x160,800x320}",
+                   "n_solves": args.n_solves, "max_steps": args.max_steps,
+                   "teams": len(plan.team_blocks), "blocks": plan.blocks},
+        "vs_baseline": None,
+        "cell_updates_per_s": cells / (res.device_ms * 1e-3),
+        "converged": int(res.converged.sum()),
+        "p50_solve_ms": float(np.percentile(res.solve_ms, 50)),
+        "p99_solve_ms": float(np.percentile(res.solve_ms, 99)),
+        "device_ms": res.device_ms,
+        "plan": {"team_blocks": plan.team_blocks},
+        "autotune_us_per_step": {f"{k[0]}x{k[1]}": v for k, v in tuner.table.items()},
+    }
+    batch.close()
+    for s in solvers:
+        s.close()
+    return line
+
+
 def run_profile(args):
     """Lean run for profilers: the exact first step, --warmup graph steps, then
     --steps eagerly launched steps (interior + boundary kernel each)."""
@@ -366,6 +436,11 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.profile:
         run_profile(args)
+        return
+    if args.workload != "plain":
+        if rank == 0:
+            line = run_warmstart(args) if args.workload == "warmstart" else run_batch(args)
+            print(json.dumps(line))
         return
     if args.impl == "reference":
         line = run_reference(args, rank, world)
