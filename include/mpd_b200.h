@@ -295,6 +295,16 @@ int mpd_nn_mse(const float *pred, const float *target, long long n, float *grad,
 int mpd_nn_adam(float *p, const float *g, float *m, float *v, long long n, float lr, float b1,
                 float b2, float eps, int step, void *stream);
 
+/* ---- restart remap ---------------------------------------------------------- */
+/* VtkIC::Apply + Impl::Interp (src/ics/vtk_ic.cpp:137-239) on the device:
+ * d_src holds 8 point fields of a snapshot (rho, v_z, v_r, v_phi, H_z, H_r,
+ * H_phi, e), ni x nj points each, point (i, j) at i + j ni; the interior cells
+ * of the 10 dense physical planes d_out10 ((L_max+2) x (M_max+3), Fields
+ * member order) receive the bilinear remap with the reference's index
+ * mapping, p and P derived.  Asynchronous on `stream`. */
+int mpd_remap_snapshot(const double *d_src, int ni, int nj, int L_max, int M_max, double gamma,
+                       double *d_out10, void *stream);
+
 /* ---- host-side expression initial condition ---------------------------------- */
 /* ExpressionIC::Apply, src/ics/expression_ic.cpp:286-324, evaluated on the host
  * with the library's expression compiler.  exprs: 8 strings in the

@@ -51,7 +51,7 @@ def build_lib(force: bool = False, verbose: bool = False) -> pathlib.Path:
     if not force and not _stale(LIB):
         return LIB
     cmd = [_nvcc(), *ARCH, *COMMON, "-shared", "-o", str(LIB),
-           *_sources("mpd_abi.cu", "noalloc.cu", "nn_gemm.cu", "nn_ops.cu", "bc_compile.cpp", "expr.cpp",
+           *_sources("mpd_abi.cu", "noalloc.cu", "nn_gemm.cu", "nn_ops.cu", "remap.cu", "bc_compile.cpp", "expr.cpp",
                     "ic_host.cpp")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

@@ -268,3 +268,31 @@ def test_persistent_engine_stops_on_residual(pkg):
         solver.close()
     assert out[0] == out[1]
     assert out[0][1] and out[0][2] <= 1e-5
+
+
+def test_vtk_restart_remap_matches_oracle(pkg, tmp_path):
+    """VtkIC (device bilinear remap) against the CPU restatement of
+    src/ics/vtk_ic.cpp:137-239, bit for bit, onto the same grid and onto a
+    finer one; then a solver starts from it."""
+    from oracle import vtk_remap
+    case = cases.channel_case(L=40, M=16, a=0.1)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+    solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=300)
+    phys = solver.physical()
+    solver.close()
+    path = pkg.io.write_vtk(tmp_path / "step_0300.vtk", phys, case.grid.r, cfg.dz, cfg.L_max,
+                            cfg.M_max)
+    ic = pkg.io.VtkIC(path)
+    src = ic.source_fields(ic.snap)
+    ni, nj = ic.snap["dims"]
+    for L, M in ((40, 16), (97, 33)):
+        fine = cases.channel_config(L=L, M=M, a=0.1)
+        fgrid = cases.make_case(fine).grid
+        got = ic.Apply(fgrid, fine)
+        want = vtk_remap.remap(src, ni, nj, L, M, fine.gamma)
+        np.testing.assert_array_equal(got, want)
+    s2 = pkg.GpuSolver(fine, fgrid, ic, precision="fast")
+    r = s2.run(T=1e300, dt=0.0, adaptive=True, max_steps=50)
+    assert r.steps == 50 and r.status == 0
+    s2.close()
