@@ -261,7 +261,9 @@ int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *
  * on the tcgen05 tensor cores:
  *   C[b](m,n) = alpha * sum_k A[b](m,k) B[b](n,k) + beta * C[b](m,n)
  * with element strides per operand (row, k, batch) so transposed operands
- * need no copy.  beta == 0 never reads C.  Launches on `stream` and returns
+ * need no copy.  beta == 0 never reads C.  With work, a GEMM of few output
+ * tiles and long K is split over K and the partials summed in a fixed order
+ * (deterministic).  Launches on `stream` and returns
  * at once; mpd_nn_wait_status synchronises the stream and reports a tensor-
  * core wait that gave up (MPD_ERR_TIMEOUT). */
 typedef struct mpd_gemm_desc {
@@ -273,6 +275,8 @@ typedef struct mpd_gemm_desc {
     float *C;
     long long scm, scn, scb;
     float alpha, beta;
+    float *work;           /* optional scratch for split-K partial sums (or NULL) */
+    long long work_floats; /* its size; K is split only when the tiles are few  */
 } mpd_gemm_desc;
 
 int mpd_nn_gemm(const mpd_gemm_desc *d, void *stream);
@@ -280,14 +284,16 @@ int mpd_nn_wait_status(void *stream);
 
 /* Element-wise and reduction kernels of the network (FP32, deterministic sums):
  * z += bias (per column), out = GELU(z) (act != 0) or z;  g_z = g_out GELU'(z);
- * out[c] = sum over rows of x[r][c];  out (+)= sum of nparts arrays of n;
+ * out[c] = sum over rows of x[r][c] (work: 128 * cols floats of scratch);
+ * out (+)= sum of nparts arrays of n;
  * mean squared error of pred vs target into *loss (one double) with
  * grad = 2 (pred - target) / n (grad may be NULL), partial = scratch of
  * 148 * 32 doubles;  one Adam step (bias-corrected, step >= 1). */
 int mpd_nn_bias_act(float *z, const float *bias, float *out, long long rows, int cols, int act,
                     void *stream);
 int mpd_nn_act_bwd(const float *g_out, const float *z, float *g_z, long long n, void *stream);
-int mpd_nn_colsum(const float *x, long long rows, int cols, float *out, void *stream);
+int mpd_nn_colsum(const float *x, long long rows, int cols, float *out, float *work,
+                  void *stream);
 int mpd_nn_sum_parts(const float *parts, int nparts, long long n, float *out, int accumulate,
                      void *stream);
 int mpd_nn_mse(const float *pred, const float *target, long long n, float *grad, double *partial,

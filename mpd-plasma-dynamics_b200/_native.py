@@ -86,7 +86,8 @@ class GemmDesc(C.Structure):
                 ("sbb", C.c_longlong),
                 ("C", C.c_void_p), ("scm", C.c_longlong), ("scn", C.c_longlong),
                 ("scb", C.c_longlong),
-                ("alpha", C.c_float), ("beta", C.c_float)]
+                ("alpha", C.c_float), ("beta", C.c_float),
+                ("work", C.c_void_p), ("work_floats", C.c_longlong)]
 
 
 class MpdError(RuntimeError):
@@ -134,7 +135,7 @@ SIGNATURES = [
     ("mpd_nn_wait_status", C.c_int, [_VP]),
     ("mpd_nn_bias_act", C.c_int, [_VP, _VP, _VP, C.c_longlong, C.c_int, C.c_int, _VP]),
     ("mpd_nn_act_bwd", C.c_int, [_VP, _VP, _VP, C.c_longlong, _VP]),
-    ("mpd_nn_colsum", C.c_int, [_VP, C.c_longlong, C.c_int, _VP, _VP]),
+    ("mpd_nn_colsum", C.c_int, [_VP, C.c_longlong, C.c_int, _VP, _VP, _VP]),
     ("mpd_nn_sum_parts", C.c_int, [_VP, C.c_int, C.c_longlong, _VP, C.c_int, _VP]),
     ("mpd_nn_mse", C.c_int, [_VP, _VP, C.c_longlong, _VP, _VP, _VP, _VP]),
     ("mpd_nn_adam", C.c_int, [_VP, _VP, _VP, _VP, C.c_longlong, C.c_float, C.c_float, C.c_float,

@@ -103,65 +103,78 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// 8 consecutive-k elements of one operand row as BF16, packed for one
-// 16-byte core-matrix row (element e in bytes 2e..2e+1).
-__device__ __forceinline__ uint4 load8_bf16(const float *p, long long sk, int kvalid) {
-    float f[8];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) f[e] = e < kvalid ? __ldg(p + (long long)e * sk) : 0.0f;
-    uint4 out;
-    __nv_bfloat162 h;
-    h = __floats2bfloat162_rn(f[0], f[1]);
-    out.x = *reinterpret_cast<uint32_t *>(&h);
-    h = __floats2bfloat162_rn(f[2], f[3]);
-    out.y = *reinterpret_cast<uint32_t *>(&h);
-    h = __floats2bfloat162_rn(f[4], f[5]);
-    out.z = *reinterpret_cast<uint32_t *>(&h);
-    h = __floats2bfloat162_rn(f[6], f[7]);
-    out.w = *reinterpret_cast<uint32_t *>(&h);
-    return out;
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&h);
 }
 
-// Stage rows [r0, r0 + ROWS) x k [k0, k0 + 64) of an operand into the
-// core-matrix layout: chunk c (8 k) of row group g at (c * ROWS/8 + g) * 128.
+// Stage rows [r0, r0 + ROWS) x k [k0, k1) of an operand into the core-matrix
+// layout: chunk c (8 k) of row group g at (c * ROWS/8 + g) * 128 bytes, row
+// r & 7 at 16 (r & 7), element e at 2 e.  All of a thread's loads are issued
+// before any is converted; rows with 16-byte aligned K-contiguous data take
+// two float4 loads per 8 elements.
 template <int ROWS>
 __device__ __forceinline__ void stage(unsigned char *dst, const float *base, long long sr,
-                                      long long sk, int nrows, int K, int r0, int k0) {
+                                      long long sk, int nrows, int k1, int r0, int k0,
+                                      bool vec) {
     constexpr int kUnits = ROWS * (kTileK / 8);
+    constexpr int kPer = kUnits / kGemmThreads;
     const bool k_contig = sk == 1;
-    for (int u = threadIdx.x; u < kUnits; u += kGemmThreads) {
-        int rl, c;
-        if (k_contig) {
-            c = u & 7;
-            rl = u >> 3;
-        } else {
-            rl = u % ROWS;
-            c = u / ROWS;
-        }
+    float f[kPer][8];
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int u = threadIdx.x + i * kGemmThreads;
+        const int rl = k_contig ? (u >> 3) : (u % ROWS);
+        const int c = k_contig ? (u & 7) : (u / ROWS);
         const int r = r0 + rl, k = k0 + 8 * c;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (r < nrows && k < K) v = load8_bf16(base + (long long)r * sr + (long long)k * sk, sk, K - k);
+        const float *p = base + (long long)r * sr + (long long)k * sk;
+        if (r < nrows && k + 8 <= k1 && vec) {
+            const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
+            const float4 b = __ldg(reinterpret_cast<const float4 *>(p) + 1);
+            f[i][0] = a.x; f[i][1] = a.y; f[i][2] = a.z; f[i][3] = a.w;
+            f[i][4] = b.x; f[i][5] = b.y; f[i][6] = b.z; f[i][7] = b.w;
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                f[i][e] = (r < nrows && k + e < k1) ? __ldg(p + (long long)e * sk) : 0.0f;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int u = threadIdx.x + i * kGemmThreads;
+        const int rl = k_contig ? (u >> 3) : (u % ROWS);
+        const int c = k_contig ? (u & 7) : (u / ROWS);
+        uint4 v;
+        v.x = pack_bf16(f[i][0], f[i][1]);
+        v.y = pack_bf16(f[i][2], f[i][3]);
+        v.z = pack_bf16(f[i][4], f[i][5]);
+        v.w = pack_bf16(f[i][6], f[i][7]);
         *reinterpret_cast<uint4 *>(dst + (c * (ROWS / 8) + (rl >> 3)) * 128 + (rl & 7) * 16) = v;
     }
 }
 
-// The two tiles in dynamic shared memory (24 KB per block).
-constexpr int kASpan = kABytes;
-constexpr int kBSpan = kBBytes;
-constexpr int kGemmSmem = kASpan + kBSpan;
-static_assert(kABytes <= kASpan && kBBytes <= kBSpan, "tile spans");
+// Two stages of tiles in dynamic shared memory (48 KB per block): the tiles
+// of chunk k+1 are staged while the tensor core works on chunk k.
+constexpr int kStageBytes = kABytes + kBBytes;
+constexpr int kGemmSmem = 2 * kStageBytes;
 
-__global__ void __launch_bounds__(kGemmThreads) nn_gemm_kernel(const mpd_gemm_desc d) {
+// C tile (m0, n0) of batch b over K range [k_begin, k_end).  With ksplit > 1
+// the raw FP32 sums go to work (split s of batch b: dense M x N at
+// ((s * batch + b) * M * N)) and nn_gemm_reduce_kernel finishes C.
+__global__ void __launch_bounds__(kGemmThreads) nn_gemm_kernel(const mpd_gemm_desc d, int ksplit,
+                                                               int kspan) {
     extern __shared__ __align__(1024) unsigned char gemm_smem[];
-    unsigned char *sA = gemm_smem;
-    unsigned char *sB = gemm_smem + kASpan;
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t tmem_slot;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * kTileN, b = blockIdx.z;
+    const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * kTileN;
+    const int b = blockIdx.z % d.batch, split = blockIdx.z / d.batch;
+    const int k_begin = split * kspan;
+    const int k_end = min(d.K, k_begin + kspan);
     const float *A = d.A + (long long)b * d.sab;
     const float *B = d.B + (long long)b * d.sbb;
-    float *C = d.C + (long long)b * d.scb;
+    const bool vec_a = d.sak == 1 && (d.sam % 4) == 0 && ((uintptr_t)A & 15) == 0;
+    const bool vec_b = d.sbk == 1 && (d.sbn % 4) == 0 && ((uintptr_t)B & 15) == 0;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -171,24 +184,35 @@ __global__ void __launch_bounds__(kGemmThreads) nn_gemm_kernel(const mpd_gemm_de
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        mbar_init(smem_addr(&bar), 1);
+        mbar_init(smem_addr(&bar[0]), 1);
+        mbar_init(smem_addr(&bar[1]), 1);
         mbar_init_fence();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    const uint32_t a_addr = smem_addr(sA), b_addr = smem_addr(sB);
 
     bool ok = true;
-    const int nchunks = (d.K + kTileK - 1) / kTileK;
+    const int nchunks = k_end > k_begin ? (k_end - k_begin + kTileK - 1) / kTileK : 0;
     for (int kc = 0; kc < nchunks; ++kc) {
-        stage<kTileM>(sA, A, d.sam, d.sak, d.M, d.K, m0, kc * kTileK);
-        stage<kTileN>(sB, B, d.sbn, d.sbk, d.N, d.K, n0, kc * kTileK);
+        const int buf = kc & 1;
+        unsigned char *sA = gemm_smem + buf * kStageBytes;
+        unsigned char *sB = sA + kABytes;
+        if (kc >= 2) {
+            // the MMAs of chunk kc - 2 read this stage: wait for their commit
+            const bool arrived = mbar_wait_bounded(smem_addr(&bar[buf]), ((kc - 2) >> 1) & 1);
+            ok = __syncthreads_and(arrived);
+            if (!ok) break;
+        }
+        const int k0 = k_begin + kc * kTileK;
+        stage<kTileM>(sA, A, d.sam, d.sak, d.M, k_end, m0, k0, vec_a);
+        stage<kTileN>(sB, B, d.sbn, d.sbk, d.N, k_end, n0, k0, vec_b);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (threadIdx.x == 0) {
             tc_fence_after();
+            const uint32_t a_addr = smem_addr(sA), b_addr = smem_addr(sB);
 #pragma unroll
             for (int s = 0; s < kTileK / 16; ++s) {
                 // K slice s = core-matrix chunks 2s, 2s+1
@@ -198,32 +222,43 @@ __global__ void __launch_bounds__(kGemmThreads) nn_gemm_kernel(const mpd_gemm_de
                                               (kTileN / 8) * 128, 128);
                 mma_bf16(tmem, ad, bd, (kc > 0 || s > 0) ? 1u : 0u);
             }
-            mma_commit(smem_addr(&bar));
+            mma_commit(smem_addr(&bar[buf]));
         }
-        // the tiles may be overwritten once the MMAs that read them are done
-        const bool arrived = mbar_wait_bounded(smem_addr(&bar), kc & 1);
-        ok = __syncthreads_and(arrived);
-        if (!ok) break;
+    }
+    if (ok && nchunks > 0) {
+        // commits complete in order: the last one covers every MMA
+        const int last = nchunks - 1;
+        ok = __syncthreads_and(mbar_wait_bounded(smem_addr(&bar[last & 1]), (last >> 1) & 1));
     }
     tc_fence_after();
-    if (ok && nchunks > 0) {
+    if (ok) {
         const int m = m0 + warp * 32 + lane;
+        float *C = d.C + (long long)b * d.scb;
+        float *W = ksplit > 1 ? d.work + ((long long)split * d.batch + b) * d.M * d.N : nullptr;
 #pragma unroll
         for (int j = 0; j < kTileN / 16; ++j) {
             float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(16 * j), v);
+            if (nchunks > 0) {
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(16 * j), v);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) v[i] = 0.0f;
+            }
             if (m < d.M) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
                     const int n = n0 + 16 * j + i;
-                    if (n < d.N) {
+                    if (n >= d.N) continue;
+                    if (W) {
+                        W[(long long)m * d.N + n] = v[i];
+                    } else {
                         float *c = C + (long long)m * d.scm + (long long)n * d.scn;
                         *c = d.beta == 0.0f ? d.alpha * v[i] : d.alpha * v[i] + d.beta * *c;
                     }
                 }
             }
         }
-    } else if (!ok && threadIdx.x == 0) {
+    } else if (threadIdx.x == 0) {
         atomicExch(&g_gemm_wait_fail, 1);
     }
     tc_fence_before();
@@ -233,6 +268,21 @@ __global__ void __launch_bounds__(kGemmThreads) nn_gemm_kernel(const mpd_gemm_de
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                      "r"(kTmemCols)
                      : "memory");
+    }
+}
+
+// C = alpha * (sum of the ksplit partials, in split order) + beta * C.
+__global__ void nn_gemm_reduce_kernel(const mpd_gemm_desc d, int ksplit) {
+    const long long mn = (long long)d.M * d.N, total = mn * d.batch;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(t / mn);
+        const long long e = t % mn;
+        const int m = (int)(e / d.N), n = (int)(e % d.N);
+        float s = 0.0f;
+        for (int k = 0; k < ksplit; ++k) s += d.work[((long long)k * d.batch + b) * mn + e];
+        float *c = d.C + (long long)b * d.scb + (long long)m * d.scm + (long long)n * d.scn;
+        *c = d.beta == 0.0f ? d.alpha * s : d.alpha * s + d.beta * *c;
     }
 }
 
@@ -254,7 +304,28 @@ int mpd_nn_gemm(const mpd_gemm_desc *d, void *stream) {
         mpd::SetLastError("mpd_nn_gemm: batch or N too large for one launch");
         return MPD_ERR_INVALID;
     }
-    const dim3 grid((d->M + kTileM - 1) / kTileM, (d->N + kTileN - 1) / kTileN, d->batch);
+    // split K when the tiles alone leave most SMs idle and the caller gave
+    // room for the partial sums (summed in split order afterwards)
+    const long long tiles = (long long)((d->M + kTileM - 1) / kTileM) *
+                            ((d->N + kTileN - 1) / kTileN) * d->batch;
+    int ksplit = 1;
+    if (d->work && tiles < 296 && d->K >= 4 * kTileK) {
+        long long want = (296 + tiles - 1) / tiles;
+        const long long by_k = d->K / (2 * kTileK);
+        const long long by_room = d->work_floats / ((long long)d->M * d->N * d->batch);
+        want = want < by_k ? want : by_k;
+        want = want < by_room ? want : by_room;
+        want = want < 64 ? want : 64;
+        if (want > 1) ksplit = (int)want;
+    }
+    const int kspan = ((d->K + ksplit - 1) / ksplit + kTileK - 1) / kTileK * kTileK;
+    ksplit = (d->K + kspan - 1) / kspan;
+    if ((long long)d->batch * ksplit > 65535) {
+        mpd::SetLastError("mpd_nn_gemm: batch too large for one launch");
+        return MPD_ERR_INVALID;
+    }
+    const dim3 grid((d->M + kTileM - 1) / kTileM, (d->N + kTileN - 1) / kTileN,
+                    d->batch * ksplit);
     static bool attr_set = false;  // per process; the attribute is per function
     if (!attr_set) {
         const cudaError_t ea = cudaFuncSetAttribute(
@@ -265,7 +336,14 @@ int mpd_nn_gemm(const mpd_gemm_desc *d, void *stream) {
         }
         attr_set = true;
     }
-    nn_gemm_kernel<<<grid, kGemmThreads, kGemmSmem, static_cast<cudaStream_t>(stream)>>>(*d);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    nn_gemm_kernel<<<grid, kGemmThreads, kGemmSmem, st>>>(*d, ksplit, kspan);
+    if (ksplit > 1) {
+        const long long total = (long long)d->M * d->N * d->batch;
+        long long blocks = (total + 255) / 256;
+        if (blocks > 148 * 16) blocks = 148 * 16;
+        nn_gemm_reduce_kernel<<<(int)blocks, 256, 0, st>>>(*d, ksplit);
+    }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         mpd::SetLastError(std::string("mpd_nn_gemm: ") + cudaGetErrorString(e));

@@ -65,21 +65,34 @@ __global__ void act_bwd_kernel(const float *g_out, const float *z, float *g_z, l
     }
 }
 
-// out[c] = sum_r x[r][c]: block = 32 columns x 8 row strides, fixed order.
-__global__ void colsum_kernel(const float *x, long long rows, int cols, float *out) {
+// Column sums in two fixed-order stages: block (bx, by) sums rows
+// by, by + kColSlices, ... of 32 columns into work[by][c]; then one thread
+// per column adds the kColSlices partials in order.
+constexpr int kColSlices = 128;
+
+__global__ void colsum_partial_kernel(const float *x, long long rows, int cols, float *work) {
     __shared__ float part[8][33];
     const int c = blockIdx.x * 32 + (threadIdx.x & 31);
     const int ry = threadIdx.x >> 5;
     float s = 0.0f;
     if (c < cols)
-        for (long long r = ry; r < rows; r += 8) s += x[r * cols + c];
+        for (long long r = (long long)blockIdx.y * 8 + ry; r < rows; r += 8LL * kColSlices)
+            s += x[r * cols + c];
     part[ry][threadIdx.x & 31] = s;
     __syncthreads();
     if (ry == 0 && c < cols) {
         float t = 0.0f;
         for (int k = 0; k < 8; ++k) t += part[k][threadIdx.x & 31];
-        out[c] = t;
+        work[(size_t)blockIdx.y * cols + c] = t;
     }
+}
+
+__global__ void colsum_final_kernel(const float *work, int cols, float *out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float t = 0.0f;
+    for (int k = 0; k < kColSlices; ++k) t += work[(size_t)k * cols + c];
+    out[c] = t;
 }
 
 // out[i] = (accumulate ? out[i] : 0) + sum_t parts[t][i]
@@ -114,12 +127,18 @@ __global__ void mse_kernel(const float *pred, const float *target, long long n, 
     if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
 }
 
+// One block: thread t sums partials t, t + 256, ... in order, then a fixed tree.
 __global__ void sum_partials_kernel(const double *partial, int n, double scale, double *out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int i = 0; i < n; ++i) s += partial[i];
-        *out = s * scale;
+    __shared__ double red[kThreads];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += kThreads) s += partial[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = kThreads / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
     }
+    if (threadIdx.x == 0) *out = red[0] * scale;
 }
 
 // Adam: m = b1 m + (1-b1) g; v = b2 v + (1-b2) g^2;
@@ -161,12 +180,15 @@ int mpd_nn_act_bwd(const float *g_out, const float *z, float *g_z, long long n, 
     return Launched("mpd_nn_act_bwd");
 }
 
-int mpd_nn_colsum(const float *x, long long rows, int cols, float *out, void *stream) {
-    if (!x || !out || rows < 0 || cols <= 0) {
+int mpd_nn_colsum(const float *x, long long rows, int cols, float *out, float *work,
+                  void *stream) {
+    if (!x || !out || !work || rows < 0 || cols <= 0) {
         mpd::SetLastError("mpd_nn_colsum: bad arguments");
         return MPD_ERR_INVALID;
     }
-    colsum_kernel<<<(cols + 31) / 32, kThreads, 0, (cudaStream_t)stream>>>(x, rows, cols, out);
+    colsum_partial_kernel<<<dim3((cols + 31) / 32, kColSlices), kThreads, 0,
+                            (cudaStream_t)stream>>>(x, rows, cols, work);
+    colsum_final_kernel<<<(cols + 127) / 128, 128, 0, (cudaStream_t)stream>>>(work, cols, out);
     return Launched("mpd_nn_colsum");
 }
 
@@ -191,7 +213,8 @@ int mpd_nn_mse(const float *pred, const float *target, long long n, float *grad,
     }
     const int nb = Blocks(n);
     mse_kernel<<<nb, kThreads, 0, (cudaStream_t)stream>>>(pred, target, n, grad, partial);
-    sum_partials_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(partial, nb, 1.0 / (double)n, loss);
+    sum_partials_kernel<<<1, kThreads, 0, (cudaStream_t)stream>>>(partial, nb, 1.0 / (double)n,
+                                                                 loss);
     return Launched("mpd_nn_mse");
 }
 

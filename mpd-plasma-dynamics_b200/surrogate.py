@@ -163,6 +163,9 @@ class SpectralOperator:
         self.gV = torch.zeros(batch, self.Q, WIDTH, **f32)
         self.parts = torch.zeros(batch * max(WIDTH, HIDDEN) * max(WIDTH, HIDDEN), **f32)
         self.partial = torch.zeros(148 * 32, device=dev, dtype=torch.float64)
+        self.colwork = torch.zeros(128 * max(WIDTH, HIDDEN), **f32)
+        # split-K partial sums of the long-K products (grid sums, weight gradients)
+        self.work = torch.zeros(16 * batch * self.Q * WIDTH, **f32)
         self.loss = torch.zeros(1, device=dev, dtype=torch.float64)
         self.step = 0
         self.lib = N.load()
@@ -201,13 +204,15 @@ class SpectralOperator:
         B, P = self.B, self.P
         parts = self.parts[:B * k_in * n_out]
         nn.gemm(a, gz, parts, k_in, n_out, P, B, sa=(1, a.stride(0), P * a.stride(0)),
-                sb=(1, gz.stride(0), P * gz.stride(0)), sc=(n_out, 1, k_in * n_out))
+                sb=(1, gz.stride(0), P * gz.stride(0)), sc=(n_out, 1, k_in * n_out),
+                work=self.work)
         self._chk(self.lib.mpd_nn_sum_parts(C.c_void_p(parts.data_ptr()), B, k_in * n_out,
                                             C.c_void_p(dst.data_ptr()), 0, self._s()))
 
     def _colsum(self, x, dst):
         self._chk(self.lib.mpd_nn_colsum(C.c_void_p(x.data_ptr()), x.shape[0], x.shape[1],
-                                         C.c_void_p(dst.data_ptr()), self._s()))
+                                         C.c_void_p(dst.data_ptr()),
+                                         C.c_void_p(self.colwork.data_ptr()), self._s()))
 
     # --------------------------------------------------------------- forward
     def load_inputs(self, x: np.ndarray):
@@ -224,7 +229,7 @@ class SpectralOperator:
             self._linear(h, Cw, p[f"W{l}"], Cw, z)
             # V[b] = F h[b]  (Q x C)
             nn.gemm(self.F, h, self.V[l], Q, Cw, P, B, sa=(P, 1, 0), sb=(1, Cw, P * Cw),
-                    sc=(Cw, 1, Q * Cw))
+                    sc=(Cw, 1, Q * Cw), work=self.work)
             # U[b, q] = V[b, q] R[q]   (batched over q)
             nn.gemm(self.V[l], p[f"R{l}"], self.U, B, Cw, Cw, Q, sa=(Q * Cw, 1, Cw),
                     sb=(1, Cw, Cw * Cw), sc=(Q * Cw, 1, Cw))
@@ -277,7 +282,7 @@ class SpectralOperator:
             self._colsum(gz, g[f"b{l}"])
             # gU[b] = G^T gz[b]
             nn.gemm(self.G, gz, self.gU, Q, Cw, P, B, sa=(1, Q, 0), sb=(1, Cw, P * Cw),
-                    sc=(Cw, 1, Q * Cw))
+                    sc=(Cw, 1, Q * Cw), work=self.work)
             # dR[q] = sum_b V[b, q]^T gU[b, q]
             nn.gemm(self.V[l], self.gU, g[f"R{l}"], Cw, Cw, B, Q, sa=(1, Q * Cw, Cw),
                     sb=(1, Q * Cw, Cw), sc=(Cw, 1, Cw * Cw))

@@ -19,7 +19,8 @@ def ref_gemm(A, B, Cin, alpha, beta):
     return out + beta * Cin if beta != 0.0 else out
 
 
-def check(pkg, M, N, K, batch, trans_a=False, trans_b=False, alpha=1.0, beta=0.0, seed=0):
+def check(pkg, M, N, K, batch, trans_a=False, trans_b=False, alpha=1.0, beta=0.0, seed=0,
+          work=0):
     import torch
     rng = np.random.default_rng(seed)
     A = rng.standard_normal((batch, M, K)).astype(np.float32)
@@ -33,7 +34,8 @@ def check(pkg, M, N, K, batch, trans_a=False, trans_b=False, alpha=1.0, beta=0.0
     dC = torch.from_numpy(C0.copy()).cuda()
     sa = (1, M, M * K) if trans_a else (K, 1, M * K)
     sb = (1, N, N * K) if trans_b else (K, 1, N * K)
-    pkg.nn.gemm(dA, dB, dC, M, N, K, batch, sa=sa, sb=sb, alpha=alpha, beta=beta)
+    w = torch.zeros(work, dtype=torch.float32, device="cuda") if work else None
+    pkg.nn.gemm(dA, dB, dC, M, N, K, batch, sa=sa, sb=sb, alpha=alpha, beta=beta, work=w)
     pkg.nn.wait_status()
     got = dC.cpu().numpy().astype(np.float64)
     want = ref_gemm(A, B, C0, alpha, beta)
@@ -59,3 +61,11 @@ def test_transposed_operands(pkg, ta, tb):
 
 def test_alpha_beta(pkg):
     check(pkg, 140, 80, 96, 2, alpha=0.5, beta=-1.25, seed=3)
+
+
+@pytest.mark.parametrize("M,N,K,batch,ta", [(256, 64, 4100, 2, False), (64, 64, 4100, 3, True),
+                                            (200, 70, 1000, 1, False)])
+def test_split_k(pkg, M, N, K, batch, ta):
+    """Few output tiles and long K: the sum is split over K (partials summed
+    in a fixed order) and must agree with numpy like the unsplit product."""
+    check(pkg, M, N, K, batch, trans_a=ta, alpha=0.75, beta=0.5, seed=11, work=64 * M * N * batch)
