@@ -46,10 +46,12 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="lean run for ncu: warm-up, then --steps eager time steps, no extras")
     ap.add_argument("--precision", choices=("fast", "exact"), default="fast")
-    ap.add_argument("--workload", choices=("plain", "warmstart", "batch"), default="plain",
+    ap.add_argument("--workload", choices=("plain", "warmstart", "batch", "surrogate"),
+                    default="plain",
                     help="plain: the 1600x640 time step (default); warmstart: surrogate-warm-"
                          "started batched steady solves vs the plain time march; batch: the "
-                         "batched sweep of uneven grids")
+                         "batched sweep of uneven grids; surrogate: training iterations of "
+                         "the warm-start network")
     ap.add_argument("--n-train", type=int, default=2000)
     ap.add_argument("--n-eval", type=int, default=256)
     ap.add_argument("--epochs", type=int, default=60)
@@ -346,6 +348,51 @@ def run_warmstart(args):
         "vs_baseline": None, "loss_first_last": [losses[0], losses[-1]], **res}
 
 
+def run_surrogate(args):
+    """Training iterations of the warm-start network (forward, MSE, backward,
+    Adam) on random inputs: grid --grid, batch 16; --warmup untimed, --steps
+    timed with CUDA events."""
+    import numpy as np
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    S = pkg.surrogate
+    L, M = (int(v) for v in args.grid.split("x"))
+    H, W, B = L, M + 1, 16
+    net = S.SpectralOperator(H, W, B, seed=0)
+    rng = np.random.default_rng(0)
+    net.load_inputs(rng.standard_normal((B, H * W, S.N_IN)))
+    tgt = torch.from_numpy(rng.standard_normal((B * H * W, S.N_OUT)).astype(np.float32)).cuda()
+
+    def iteration():
+        net.forward()
+        net.loss_and_grad(tgt)
+        net.backward()
+        net.adam_step()
+
+    for _ in range(args.warmup):
+        iteration()
+    net.wait()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        iteration()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    P, Q, Cw = H * W, net.Q, S.WIDTH
+    # multiply-adds of one forward pass per sample; backward ~ 2x
+    fwd = P * S.N_IN * Cw + S.LAYERS * (2 * Q * P * Cw + Q * Cw * Cw + P * Cw * Cw) + \
+        P * Cw * S.HIDDEN + P * S.HIDDEN * S.N_OUT
+    flops = 2 * 3 * fwd * B
+    return {"metric": "surrogate training iteration", "value": ms, "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "dtype": "bf16 operands, f32 accumulate", "data": "synthetic (random)",
+            "config": {"workload": f"spectral operator on {L}x{M}, batch {B}",
+                       "parameters": net.nparam},
+            "vs_baseline": None, "gemm_tflops": flops / (ms * 1e-3) / 1e12}
+
+
 def run_batch(args):
     """The batched sweep: n solves drawn from the sweep box (uneven grids),
     autotuned teams, one persistent cooperative launch, cold start."""
@@ -439,7 +486,9 @@ def main():
         return
     if args.workload != "plain":
         if rank == 0:
-            line = run_warmstart(args) if args.workload == "warmstart" else run_batch(args)
+            runner = {"warmstart": run_warmstart, "batch": run_batch,
+                      "surrogate": run_surrogate}[args.workload]
+            line = runner(args)
             print(json.dumps(line))
         return
     if args.impl == "reference":
