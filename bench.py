@@ -46,18 +46,24 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="lean run for ncu: warm-up, then --steps eager time steps, no extras")
     ap.add_argument("--precision", choices=("fast", "exact"), default="fast")
-    ap.add_argument("--workload", choices=("plain", "warmstart", "batch", "surrogate"),
+    ap.add_argument("--workload", choices=("plain", "warmstart", "batch", "surrogate", "serve"),
                     default="plain",
                     help="plain: the 1600x640 time step (default); warmstart: surrogate-warm-"
                          "started batched steady solves vs the plain time march; batch: the "
                          "batched sweep of uneven grids; surrogate: training iterations of "
-                         "the warm-start network")
+                         "the warm-start network; serve: a large warm-started grid beside a "
+                         "memory-budgeted batch of small solves")
     ap.add_argument("--n-train", type=int, default=2000)
     ap.add_argument("--n-eval", type=int, default=256)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--grid", type=str, default="100x40")
     ap.add_argument("--n-solves", type=int, default=64)
     ap.add_argument("--max-steps", type=int, default=200000)
+    ap.add_argument("--surrogate", type=str, default="",
+                    help="trained surrogate (.npz from --workload warmstart --save); "
+                         "without it serve trains a small one first")
+    ap.add_argument("--save", type=str, default="", help="warmstart: save the surrogate here")
+    ap.add_argument("--big", type=str, default="4096x1600")
     return ap.parse_args()
 
 
@@ -335,7 +341,8 @@ def run_warmstart(args):
     L, M = (int(v) for v in args.grid.split("x"))
     res = pkg.warmstart.run_pipeline(n_train=args.n_train, n_eval=args.n_eval, grid=(L, M),
                                      epochs=args.epochs, max_steps=args.max_steps,
-                                     log=lambda m: print(m, file=sys.stderr, flush=True))
+                                     log=lambda m: print(m, file=sys.stderr, flush=True),
+                                     save=args.save or None)
     losses = res.pop("losses")
     return {
         "metric": "steady solves/s, warm-start batch (residual <= 1e-8)",
@@ -346,6 +353,38 @@ def run_warmstart(args):
                    "n_train": args.n_train, "n_eval": args.n_eval, "epochs": args.epochs,
                    "surrogate": "4 spectral layers, 64 channels, 8 modes per axis"},
         "vs_baseline": None, "loss_first_last": [losses[0], losses[-1]], **res}
+
+
+def run_serve(args):
+    """Config 5 of the north star, bounded: a large converging-diverging
+    channel warm-started from the surrogate (coarse prediction remapped on
+    the device) in one persistent launch beside small sweep solves admitted by
+    a device-memory budget; the same mix cold for comparison."""
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    WS = pkg.warmstart
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    if args.surrogate:
+        tr = WS.Trained.load(args.surrogate)
+    else:
+        L, M = (int(v) for v in args.grid.split("x"))
+        params = WS.draws(range(args.n_train), (L, M))
+        data = WS.solve_all(params, max_steps=args.max_steps)
+        keep = [i for i in range(len(params)) if data.converged[i]]
+        g = WS.grid_of(params[0].config())
+        import numpy as np
+        X = np.stack([WS.inputs_of(params[i], g) for i in keep])
+        Y = np.stack([data.fields[i].reshape(-1, 8) for i in keep])
+        tr = WS.train(X, Y, L, M + 1, epochs=args.epochs, log=log)
+    bL, bM = (int(v) for v in args.big.split("x"))
+    res = pkg.serve.run_serving(tr, big=(bL, bM), n_small=args.n_solves,
+                                max_steps=min(args.max_steps, args.steps), log=log)
+    return {"metric": "serving mix: small solves/s beside a warm-started large grid",
+            "value": res["warm"]["small_solves_per_s"], "unit": "solves/s",
+            "higher_is_better": True, "n_gpus": 1, "dtype": "f64", "vs_baseline": None,
+            "data": "synthetic (sweep-box draws)",
+            "config": {"workload": f"large channel {args.big} a=0.3 + {args.n_solves} small",
+                       "steps_cap": min(args.max_steps, args.steps)}, **res}
 
 
 def run_surrogate(args):
@@ -487,7 +526,7 @@ def main():
     if args.workload != "plain":
         if rank == 0:
             runner = {"warmstart": run_warmstart, "batch": run_batch,
-                      "surrogate": run_surrogate}[args.workload]
+                      "surrogate": run_surrogate, "serve": run_serve}[args.workload]
             line = runner(args)
             print(json.dumps(line))
         return

@@ -248,12 +248,13 @@ void mpd_batch_destroy(mpd_batch *b);
 int mpd_batch_capacity(mpd_batch *b, int *blocks);
 /* Run every solve with the same run parameters (convergence_threshold must be
  * 0; steps_per_graph = steps each solve may take per launch, 0 = 5000).
- * stats: n entries.  solve_ms (n entries, or NULL): time from the first step
+ * dt0 (n entries, or NULL for p->dt): each solve's initial dt (<= 0: the CFL
+ * limit of its state).  stats: n entries.  solve_ms (n entries, or NULL): time from the first step
  * any solve took in this run to this solve's last step.  device_ms (or NULL):
  * the whole run. */
 int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *team_blocks,
-                  const int *solve_team, mpd_run_stats *stats, double *solve_ms,
-                  double *device_ms);
+                  const int *solve_team, const double *dt0, mpd_run_stats *stats,
+                  double *solve_ms, double *device_ms);
 
 /* ---- surrogate network kernels (learned warm start) -------------------------- */
 /* New; the reference has no learned component.  Device pointers, FP32 in

@@ -7,7 +7,7 @@ The compute path is the CUDA library ``libmpd_b200.so`` behind the C ABI of
 conditions (``ic``), the solver handle (``solver``), batched solves and their
 autotuner (``batch``).
 """
-from . import _native, io, nn, surrogate, warmstart, workloads
+from . import _native, io, nn, serve, surrogate, warmstart, workloads
 from .config import BCSegmentConfig, ConfigError, FieldCond, SimConfig, segment
 from .geometry import GeometryRegistry, Grid, IGeometry, register_all_geometries
 from .ic import ArrayIC, ExpressionIC, IInitialCondition

@@ -130,7 +130,7 @@ SIGNATURES = [
     ("mpd_batch_destroy", None, [_VP]),
     ("mpd_batch_capacity", C.c_int, [_VP, C.POINTER(C.c_int)]),
     ("mpd_batch_run", C.c_int, [_VP, C.POINTER(RunParams), C.c_int, C.POINTER(C.c_int),
-                                C.POINTER(C.c_int), C.POINTER(RunStats), DP, DP]),
+                                C.POINTER(C.c_int), DP, C.POINTER(RunStats), DP, DP]),
     ("mpd_nn_gemm", C.c_int, [C.POINTER(GemmDesc), _VP]),
     ("mpd_nn_wait_status", C.c_int, [_VP]),
     ("mpd_nn_bias_act", C.c_int, [_VP, _VP, _VP, C.c_longlong, C.c_int, C.c_int, _VP]),

@@ -95,7 +95,11 @@ class BatchSolver:
 
     def run(self, plan: BatchPlan, T: float = 1e300, dt: float | None = None,
             adaptive: bool = True, max_steps: int = 200_000, residual_tol: float = 0.0,
-            residual_every: int = 50, steps_per_launch: int = 0) -> BatchResult:
+            residual_every: int = 50, steps_per_launch: int = 0,
+            dt_per_solve=None) -> BatchResult:
+        """dt: initial dt of every solve (None: the first solver's config dt;
+        <= 0: the CFL limit of each solve's state); dt_per_solve overrides it
+        per solve."""
         cfg = self.solvers[0].cfg
         p = _params(T, cfg.dt if dt is None else dt, adaptive, cfg.cfl_number,
                     cfg.dt_growth_factor, cfg.dt_min, cfg.dt_max, max_steps, residual_tol,
@@ -108,8 +112,14 @@ class BatchSolver:
         stats = (N.RunStats * n)()
         solve_ms = np.zeros(n)
         dev_ms = C.c_double()
-        rc = self.lib.mpd_batch_run(self.h, C.byref(p), len(plan.team_blocks), tb, st, stats,
-                                    solve_ms.ctypes.data_as(N.DP), C.byref(dev_ms))
+        dts = None
+        if dt_per_solve is not None:
+            dts = np.ascontiguousarray(dt_per_solve, dtype=np.float64)
+            if dts.shape != (n,):
+                raise ValueError("dt_per_solve needs one entry per solve")
+        rc = self.lib.mpd_batch_run(self.h, C.byref(p), len(plan.team_blocks), tb, st,
+                                    dts.ctypes.data_as(N.DP) if dts is not None else None,
+                                    stats, solve_ms.ctypes.data_as(N.DP), C.byref(dev_ms))
         if rc not in (N.MPD_OK, N.MPD_ERR_NONFINITE):
             N.check(rc, self.lib)
         runs = [RunResult(s.steps, s.t, s.dt, s.residual, s.change, s.max_wave_speed,

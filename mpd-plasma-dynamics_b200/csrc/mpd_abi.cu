@@ -1001,8 +1001,8 @@ int mpd_batch_capacity(mpd_batch *b, int *blocks) {
 }
 
 int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *team_blocks,
-                  const int *solve_team, mpd_run_stats *stats, double *solve_ms,
-                  double *device_ms) {
+                  const int *solve_team, const double *dt0, mpd_run_stats *stats,
+                  double *solve_ms, double *device_ms) {
     if (!b) return Fail(MPD_ERR_INVALID, "batch handle is NULL");
     const int n = static_cast<int>(b->solvers.size());
     if (!team_blocks || !solve_team || nteams < 1 || nteams > n)
@@ -1028,7 +1028,9 @@ int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *
         mpd_solver *s = b->solvers[i];
         int rc = CheckRunParams(s, p);
         if (rc != MPD_OK) return rc;
-        rc = PrepareRun(s, p, step0[i]);
+        mpd_run_params pi = *p;
+        if (dt0) pi.dt = dt0[i];
+        rc = PrepareRun(s, &pi, step0[i]);
         if (rc != MPD_OK) return rc;
         MPD_CK(cudaEventRecord(s->ev0, s->stream));
         const bool first = !s->h_st->done && s->host_step == 0;

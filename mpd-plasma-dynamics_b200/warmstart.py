@@ -128,6 +128,20 @@ class Trained:
     losses: list
     train_s: float
 
+    def save(self, path):
+        p = self.net.get_params()
+        np.savez(path, H=self.net.H, W=self.net.W, mean=self.norm.mean, std=self.norm.std,
+                 const=self.norm.const, losses=np.array(self.losses),
+                 **{f"p_{k}": v for k, v in p.items()})
+
+    @classmethod
+    def load(cls, path, batch: int = 16) -> "Trained":
+        z = np.load(path)
+        params = {k[2:]: z[k] for k in z.files if k.startswith("p_")}
+        net = S.SpectralOperator(int(z["H"]), int(z["W"]), batch, params=params)
+        norm = S.Normalizer(z["mean"], z["std"], z["const"])
+        return cls(net, norm, list(z["losses"]), 0.0)
+
 
 def train(X: np.ndarray, Y: np.ndarray, H: int, W: int, epochs: int = 40, batch: int = 16,
           lr: float = 1e-3, seed: int = 0, log=None) -> Trained:
@@ -195,7 +209,8 @@ def relative_linf(a: np.ndarray, b: np.ndarray) -> np.ndarray:
 
 
 def run_pipeline(n_train=2000, n_eval=256, grid=(100, 40), epochs=40, batch=16, lr=1e-3,
-                 max_steps=200_000, tol=1e-8, plain_sample=4, log=print) -> dict:
+                 max_steps=200_000, tol=1e-8, plain_sample=4, log=print,
+                 save: str | None = None) -> dict:
     """Steps 1-3 of the module docstring; returns the measurements."""
     L, M = grid
     H, W = L, M + 1
@@ -212,6 +227,8 @@ def run_pipeline(n_train=2000, n_eval=256, grid=(100, 40), epochs=40, batch=16, 
     Y = np.stack([data.fields[i].reshape(H * W, S.N_OUT) for i in keep])
     tr = train(X, Y, H, W, epochs=epochs, batch=batch, lr=lr, log=log)
     log(f"trained {epochs} epochs in {tr.train_s:.1f} s, final loss {tr.losses[-1]:.3e}")
+    if save:
+        tr.save(save)
 
     Xe = np.stack([inputs_of(p, grids[0]) for p in eval_p])
     pred, infer_s = predict(tr, Xe)
