@@ -198,7 +198,7 @@ int mpd_emu_advance(void *h, double dt, int order) {
     for (int t = 0; t < nring; ++t) {
         const int i = order == 2 ? nring - 1 - t : t;
         int l, m;
-        mpd::ring_cell(g, i, l, m);
+        if (!mpd::ring_cell(g, i, l, m)) continue;
         double *uf = &ring[8 * static_cast<size_t>(i)];
         mpd::bc_ring_final(v, l, m, uf);
         if (m == 1 || m == g.M + 1)
@@ -210,7 +210,7 @@ int mpd_emu_advance(void *h, double dt, int order) {
     if (order == 0) {
         for (int i = 0; i < nring; ++i) {
             int l, m;
-            mpd::ring_cell(g, i, l, m);
+            if (!mpd::ring_cell(g, i, l, m)) continue;
             for (int k = 0; k < 8; ++k) u[k * g.ps + g.ix(l, m)] = ring[8 * static_cast<size_t>(i) + k];
         }
     }

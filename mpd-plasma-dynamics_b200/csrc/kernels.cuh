@@ -155,14 +155,15 @@ __device__ __forceinline__ void ring_prefetch(const BcView &v, int l, int m) {
     }
 }
 
-// Boundary-ring cell i of one step: its final conserved values into v.u, and
+// Boundary-ring slot i of one step (nothing for an idle slot): the cell's
+// final conserved values into v.u, and
 // the full reconstruction of the cell: its wave speed (want_ws) and, for the
 // wall columns, the "old" value the next step's faces read (wall lines wnext).
 __device__ __forceinline__ void ring_cell_update(const BcView &v, int i, double *wnext,
                                                  bool want_ws, CellStats &cs) {
     const Geo &g = v.g;
     int l, m;
-    ring_cell(g, i, l, m);
+    if (!ring_cell(g, i, l, m)) return;
     ring_prefetch(v, l, m);
     double uf[8];
     bc_ring_final(v, l, m, uf);

@@ -944,20 +944,44 @@ MPD_HD void phys_to_prim_u(const Prim &q, double r, double u[8]) {
     rebuild_u(p, r, u);
 }
 
-// Number of boundary-ring cells: rows l = 1 and l = L (m = 1..M+1) and
-// columns m = 1 and m = M+1 (l = 2..L-1).
-MPD_HD int ring_count(const Geo &g) { return 2 * (g.M + 1) + 2 * (g.L - 2); }
+// Ring slots: the edge cells of rows l = 1 and l = L (m = 2..M) and of
+// columns m = 1 and m = M+1 (l = 2..L-1), then the four corners, each at the
+// start of its own 32-slot group (the other slots of a group are idle).  The
+// corners run the longest recomputation chains; alone in their warps they do
+// not serialise behind the edge cells' code paths.
+constexpr int kRingGroup = 32;
 
-MPD_HD void ring_cell(const Geo &g, int i, int &l, int &m) {
-    const int row = g.M + 1;
-    if (i < row) { l = 1; m = 1 + i; return; }
-    i -= row;
-    if (i < row) { l = g.L; m = 1 + i; return; }
-    i -= row;
-    if (i < g.L - 2) { l = 2 + i; m = 1; return; }
-    i -= g.L - 2;
-    l = 2 + i;
-    m = g.M + 1;
+MPD_HD int ring_edges(const Geo &g) { return 2 * (g.M - 1) + 2 * (g.L - 2); }
+
+MPD_HD int ring_count(const Geo &g) {
+    const int e = ring_edges(g);
+    return (e + kRingGroup - 1) / kRingGroup * kRingGroup + 4 * kRingGroup;
+}
+
+// Cell of ring slot i; false for an idle slot.
+MPD_HD bool ring_cell(const Geo &g, int i, int &l, int &m) {
+    const int inner = g.M - 1;
+    const int e = ring_edges(g);
+    if (i < e) {
+        if (i < inner) { l = 1; m = 2 + i; return true; }
+        i -= inner;
+        if (i < inner) { l = g.L; m = 2 + i; return true; }
+        i -= inner;
+        if (i < g.L - 2) { l = 2 + i; m = 1; return true; }
+        i -= g.L - 2;
+        l = 2 + i;
+        m = g.M + 1;
+        return true;
+    }
+    const int c = i - (e + kRingGroup - 1) / kRingGroup * kRingGroup;
+    if (c < 0 || c % kRingGroup != 0) return false;
+    switch (c / kRingGroup) {
+        case 0: l = 1; m = 1; return true;
+        case 1: l = 1; m = g.M + 1; return true;
+        case 2: l = g.L; m = 1; return true;
+        case 3: l = g.L; m = g.M + 1; return true;
+        default: return false;
+    }
 }
 
 // Final conserved values of boundary-ring cell (l, m) after the four faces
