@@ -11,7 +11,9 @@ residual schedule, same bits).
 Autotuner: for every grid shape in the batch it times a scratch solve of that
 shape on a team of each candidate size (a one-team batch, CUDA events), then
 packs the batch: per shape a team size and a team count, grown greedily on
-the shape whose estimated finish time is latest, within one cooperative wave.
+the shape whose estimated finish time is latest (more teams, skipping counts
+that leave the most-loaded team's share unchanged, or larger teams, whichever
+shortens that finish most per block), within one cooperative wave.
 """
 from __future__ import annotations
 
@@ -187,15 +189,21 @@ class Autotuner:
         while True:
             k = max(state, key=lambda s: finish(s, *state[s]))
             blocks, teams = state[k]
+            n = len(shapes[k])
             now = finish(k, blocks, teams)
             free = self.capacity - used
             options = []
-            if teams < len(shapes[k]) and blocks <= free:
-                options.append((now - finish(k, blocks, teams + 1), blocks, (blocks, teams + 1)))
+            per = math.ceil(n / teams)
+            if per > 1:
+                # the fewest teams that leave each at most per - 1 solves: adding
+                # fewer changes nothing (ceil(n / teams) is flat in between)
+                nt = math.ceil(n / (per - 1))
+                if (nt - teams) * blocks <= free:
+                    options.append((now - finish(k, blocks, nt), (nt - teams) * blocks,
+                                    (blocks, nt)))
             for nb in timing[k]:
                 if nb > blocks and (nb - blocks) * teams <= free:
                     options.append((now - finish(k, nb, teams), (nb - blocks) * teams, (nb, teams)))
-                    break
             options = [o for o in options if o[0] > 0]
             if not options:
                 break

@@ -169,12 +169,13 @@ int mpd_emu_advance(void *h, double dt, int order) {
                         mpd::fast_gr(U[p], q[p], R[p], Gr[p]);
                     }
                 }
-                double A[9], B[9], ce[8], cw[8], ce_e[8], cw_w[8];
+                double A[9], B[9], S[10], ce[8], cw[8], ce_e[8], cw_w[8];
                 mpd::fast_a(U[2], Gz[2], kz, A);
                 mpd::fast_rc(U[3], Gr[3], kr, ce_e, cw);   // east neighbour's ce
                 mpd::fast_rc(U[4], Gr[4], kr, ce, cw_w);   // west neighbour's cw
                 mpd::fast_b(ce_e, cw_w, Gr[3][7], Gr[4][7], q[0], kr, dt, B);
-                mpd::fast_finish(A, B, U[1], Gz[1], kz, out);
+                mpd::fast_sum(A, B, S);
+                mpd::fast_finish(S, U[1], Gz[1], kz, out);
             }
             for (int k = 0; k < 8; ++k) u[k * g.ps + g.ix(l, m)] = out[k];
             if (mpd::wants_central(g.L, g.M, l, m))

@@ -174,7 +174,8 @@ __device__ __forceinline__ void ring_cell_update(const BcView &v, int i, double 
     if (want_ws || wall) {
         const double r = g.r(l, m);
         const Phys q = recon_bc(v, uf, r);
-        if (want_ws) cs.add_ws(v.fast ? fast_wave_speed(uf, r, g.gamma) : wave_speed(q, g.gamma));
+        if (want_ws)
+            cs.add_ws(v.fast ? fast_wave_speed(uf, r, rcp_nr(r), g.gamma) : wave_speed(q, g.gamma));
         if (wall) store_line_phys(wnext, v.len, m == 1 ? 0 : 1, l, q);
     }
 }

@@ -234,14 +234,15 @@ MPD_HD void lf_cell_exact(const double U[5][8], const Phys Q[5], const double R[
 // Newton iteration from a single-precision seed.
 // ---------------------------------------------------------------------------
 
-// 1/x for |x| in the normal single-precision range: single-precision seed
-// (relative error < 2^-22), two Newton-Raphson steps y <- y + y (1 - x y),
-// each doubling the correct bits (2^-44, then below double rounding).
+// 1/x: a seed of at least 16 correct bits, then two Newton-Raphson steps
+// y <- y + y (1 - x y), each squaring the relative error (2^-32, then below
+// double rounding).  On the device the seed is the hardware's double-precision
+// reciprocal approximation (rcp.approx.ftz.f64, from the upper word of x: no
+// conversions, any normal double); on the host a single-precision reciprocal.
 MPD_HD double rcp_nr(double x) {
 #ifdef __CUDA_ARCH__
-    float yf;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"((float)x));
-    double y = (double)yf;
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
 #else
     double y = (double)(1.0f / (float)x);
 #endif
@@ -251,19 +252,19 @@ MPD_HD double rcp_nr(double x) {
     return fma(y, e, y);
 }
 
-// sqrt(a) for a in the normal single-precision range (0 -> 0, a < 0 -> NaN):
-// single-precision 1/sqrt seed, two Newton steps y <- y (3 - a y^2) / 2, then
-// s = a y with one Heron correction s <- s + y (a - s^2) / 2.
+// sqrt(a) (0 -> 0, a < 0 -> NaN): a 1/sqrt seed y0 of at least 16 correct
+// bits, one Newton step y <- y (3 - a y^2) / 2 (relative error 1.5 e0^2 <=
+// 2^-31), then s = a y and one Heron correction s <- s + y (a - s^2) / 2, which
+// leaves a relative error of e^2 / 2 (below 2^-62).  Device seed:
+// rsqrt.approx.ftz.f64; host seed: single precision.
 MPD_HD double sqrt_nr(double a) {
 #ifdef __CUDA_ARCH__
-    float yf;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"((float)a));
-    double y = (double)yf;
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
 #else
     double y = (double)(1.0f / sqrtf((float)a));
 #endif
     const double ha = 0.5 * a;
-    y = y * fma(-ha * y, y, 1.5);
     y = y * fma(-ha * y, y, 1.5);
     const double s = a * y;
     const double r = fma(-s, s, a);
@@ -274,6 +275,7 @@ MPD_HD double sqrt_nr(double a) {
 // Primitive values of one point (Fields::UpdatePhysicalFromU with reciprocals).
 struct FastPrim {
     double rho, vz, vr, vphi, e, Hphi, Hz, Hr, p, P;
+    double ir;  // 1 / r of the point
 };
 
 MPD_HD FastPrim fast_prim(const double U[8], double r, double gm1) {
@@ -290,6 +292,7 @@ MPD_HD FastPrim fast_prim(const double U[8], double r, double gm1) {
     q.Hr = U[7] * ir;
     q.p = gm1 * q.rho * q.e;
     q.P = fma(0.5, fma(q.Hz, q.Hz, fma(q.Hr, q.Hr, q.Hphi * q.Hphi)), q.p);
+    q.ir = ir;
     return q;
 }
 
@@ -351,27 +354,36 @@ MPD_HD void fast_b(const double ce_e[8], const double cw_w[8], double g7e, doubl
     B[8] = q.p;
 }
 
-// Close cell row l with point row l+1 (U, Gz).
-MPD_HD void fast_finish(const double A[9], const double B[9], const double Un[8],
-                        const double Gzn[8], double kz, double out[8]) {
+// The running sums of cell row l once its own point row has been folded in:
+// S[k] = A[k] + B[k] (k < 8), S[8] = p (B[8]), S[9] = v_z r of the point row
+// below (A[8]).
+MPD_HD void fast_sum(const double A[9], const double B[9], double S[10]) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const double s = A[k] + B[k];
-        out[k] = (k == 6) ? fma(0.25, Un[6], s) : fma(kz, Gzn[k], fma(0.25, Un[k], s));
-    }
-    // z part of u_5's source: -p kz ((v_z r)_n - (v_z r)_s)
-    out[4] = fma(-B[8] * kz, Gzn[6] - A[8], out[4]);
+    for (int k = 0; k < 8; ++k) S[k] = A[k] + B[k];
+    S[8] = B[8];
+    S[9] = A[8];
 }
 
-// Wave speed |v| + c_s + c_a of a new cell state (reciprocals, Newton sqrt).
-MPD_HD double fast_wave_speed(const double u[8], double r, double gamma) {
-    const double ir = rcp_nr(r), iu = rcp_nr(u[0]);
-    const double rho = u[0] * ir, vz = u[1] * iu, vr = u[2] * iu;
-    const double e = u[4] * iu, Hphi = u[5], Hz = u[6] * ir, Hr = u[7] * ir;
-    const double prs = (gamma - 1.0) * rho * e;
-    const double irho = r * iu;
-    const double cs2 = gamma * prs * irho;
-    const double ca2 = fma(Hz, Hz, fma(Hr, Hr, Hphi * Hphi)) * irho;
+// Close cell row l (sums S) with point row l+1 (U, Gz).
+MPD_HD void fast_finish(const double S[10], const double Un[8], const double Gzn[8], double kz,
+                        double out[8]) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        out[k] = (k == 6) ? fma(0.25, Un[6], S[k]) : fma(kz, Gzn[k], fma(0.25, Un[k], S[k]));
+    // z part of u_5's source: -p kz ((v_z r)_n - (v_z r)_s)
+    out[4] = fma(-S[8] * kz, Gzn[6] - S[9], out[4]);
+}
+
+// Wave speed |v| + c_s + c_a of a new cell state at radius r (ir = 1 / r),
+// with reciprocals and Newton square roots:
+//   |v|^2 = (u_2^2 + u_3^2) / u_1^2,  c_s^2 = gamma (gamma - 1) u_5 / u_1,
+//   c_a^2 = (H_z^2 + H_r^2 + H_phi^2) r / u_1   (u_1 = rho r, u_5 = rho e r).
+MPD_HD double fast_wave_speed(const double u[8], double r, double ir, double gamma) {
+    const double iu = rcp_nr(u[0]);
+    const double vz = u[1] * iu, vr = u[2] * iu;
+    const double Hz = u[6] * ir, Hr = u[7] * ir, Hphi = u[5];
+    const double cs2 = gamma * (gamma - 1.0) * u[4] * iu;
+    const double ca2 = fma(Hz, Hz, fma(Hr, Hr, Hphi * Hphi)) * (r * iu);
     const double v2 = fma(vz, vz, vr * vr);
     return sqrt_nr(v2) + sqrt_nr(cs2) + sqrt_nr(ca2);
 }

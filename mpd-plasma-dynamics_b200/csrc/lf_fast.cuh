@@ -7,11 +7,14 @@
 //     lanes 0 and 31 are the strip's halo points) and marches down the rows
 //     of its band, receiving each row of the 8 conserved planes once;
 //   * every point is evaluated once (fast_prim / fast_gz / fast_gr) and folded
-//     into two running sums: A for the cell row below it, B (with the r
-//     neighbours taken from the adjacent lanes by warp shuffles) for its own
-//     cell row; a cell row is closed when the point row after it arrives
-//     (fast_finish), so only 27 doubles of state cross iterations;
-//   * divides are Newton reciprocals from a single-precision seed.
+//     into two running sums: A for the cell row below it and, with the r
+//     neighbours taken from the adjacent lanes by warp shuffles, B for its own
+//     cell row, which is added to that row's A at once (S = A + B); a cell row
+//     is closed when the point row after it arrives (fast_finish), so only 19
+//     doubles of state (A of the next row, S of the current one) cross rows;
+//   * divides are Newton reciprocals from the hardware's approximate seed;
+//   * a row's geometry (r profiles, dr) is loaded before its conserved values
+//     are waited for, so those loads overlap the wait.
 // The result differs from the exact kernel by rounding only (checked against
 // the oracle at <= 1e-12 relative L-inf after 1000 steps).  Fused: the new
 // state's maximum wave speed (adaptive dt) and the NaN/Inf sentinel.
@@ -25,6 +28,11 @@ namespace mpd {
 
 constexpr int kFastCells = 30;  // output columns per warp
 
+// Geometry of one point row: the wall radii and the row's dr.
+struct RowGeo {
+    double rin, rout, dr;
+};
+
 struct FastStrip {
     Geo g;
     double *__restrict__ u;
@@ -36,20 +44,22 @@ struct FastStrip {
     bool out_lane;   // lane writes a cell
     double frac, gm1, kz, dt;
 
-    __device__ __forceinline__ double radius(int l) const {
-        return (1.0 - frac) * g.rin[l] + frac * g.rout[l];
+    __device__ __forceinline__ RowGeo row_geo(int n) const {
+        return RowGeo{__ldg(g.rin + n), __ldg(g.rout + n), __ldg(g.dr + n)};
+    }
+    __device__ __forceinline__ double radius(const RowGeo &rg) const {
+        return (1.0 - frac) * rg.rin + frac * rg.rout;
     }
     __device__ __forceinline__ bool ghost(int l) const { return !pvalid || l <= 0 || l >= g.L + 1; }
 
-    // Point row n's contributions: A[] for the cell row below it and, when
-    // row n is a cell row of this strip (with_b, warp-uniform), B[] for itself.
-    // U must be zero on ghost points (the row staging guarantees it).  The shuffles sit
-    // outside every lane-dependent branch: all 32 lanes take part.
-    __device__ __forceinline__ void point(int n, const double U[8], const FastPrim &q, double r,
-                                          const double Gz[8], bool gh, bool with_b, double A[9],
-                                          double B[9]) const {
-        fast_a(U, Gz, kz, A);
-        if (!with_b) return;
+    // Point row n, a cell row of this strip: its B (the r neighbours' shares
+    // by warp shuffles, its own sources) folded with the row's A into S, then
+    // A replaced by the A this point row gives the cell row below it.  U must
+    // be zero on ghost points (the row staging guarantees it).  The shuffles
+    // sit outside every lane-dependent branch: all 32 lanes take part.
+    __device__ __forceinline__ void point(const RowGeo &rg, const double U[8], const FastPrim &q,
+                                          double r, const double Gz[8], bool gh, double A[9],
+                                          double S[10]) const {
         double Gr[8];
         if (gh) {
 #pragma unroll
@@ -58,7 +68,8 @@ struct FastStrip {
             fast_gr(U, q, r, Gr);
         }
         // fast_rc + fast_b, each equation's two shuffles folded in as they arrive
-        const double kr = dt * (0.5 / g.dr[n]);
+        const double kr = dt * (0.5 / rg.dr);
+        double B[9];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const double q4 = 0.25 * U[k];
@@ -72,11 +83,13 @@ struct FastStrip {
         B[3] = fma(dt, fma(-q.rho * q.vr, q.vphi, q.Hphi * q.Hr), B[3]);
         B[4] = fma(-q.p * kr, d7, B[4]);
         B[8] = q.p;
+        fast_sum(A, B, S);
+        fast_a(U, Gz, kz, A);
     }
 
     // Primitives and z fluxes of point row n (zeros on ghost points).
-    __device__ __forceinline__ bool eval(int n, const double U[8], FastPrim &q, double &r,
-                                         double Gz[8]) const {
+    __device__ __forceinline__ bool eval(int n, const RowGeo &rg, const double U[8], FastPrim &q,
+                                         double &r, double Gz[8]) const {
         const bool gh = ghost(n);
         if (gh) {
             q = FastPrim{};
@@ -84,7 +97,7 @@ struct FastStrip {
 #pragma unroll
             for (int k = 0; k < 8; ++k) Gz[k] = 0.0;
         } else {
-            r = radius(n);
+            r = radius(rg);
             q = fast_prim(U, r, gm1);
             fast_gz(U, q, r, Gz);
         }

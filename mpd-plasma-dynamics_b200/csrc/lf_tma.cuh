@@ -95,20 +95,24 @@ struct TmaWarp {
     }
 };
 
+// Close cell row l (sums S) with point row n = l + 1 and fold that point row
+// in: S and A move on to row n.  r_l / ir_l: radius of row l and its
+// reciprocal (from the evaluation of point row l), replaced by row n's.
 template <bool WANT_WS>
 __device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, int l_end, uint32_t &j,
-                                        double Acur[9], double B[9], unsigned long long &ws_key,
-                                        unsigned int &nf) {
+                                        double A[9], double S[10], double &r_l, double &ir_l,
+                                        unsigned long long &ws_key, unsigned int &nf) {
     const FastStrip &s = w.f;
-    const int n = l + 1;  // point row n closes cell row l
+    const int n = l + 1;
+    const RowGeo rg = s.row_geo(n);  // issued before the wait, so the loads overlap it
     double Un[8];
     if (!w.take(j, Un)) return false;
     FastPrim q;
     double r, Gz[8], out[8];
-    const bool gh = s.eval(n, Un, q, r, Gz);
+    const bool gh = s.eval(n, rg, Un, q, r, Gz);
     w.release(j);
     ++j;
-    fast_finish(Acur, B, Un, Gz, s.kz, out);
+    fast_finish(S, Un, Gz, s.kz, out);
     if (s.out_lane) {
         const Geo &g = s.g;
         const size_t i = g.ix(l, s.p);
@@ -116,13 +120,15 @@ __device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, int l_end, uint
         for (int k = 0; k < 8; ++k) s.u[(size_t)k * g.ps + i] = out[k];
         if (wants_central(g.L, g.M, l, s.p)) store_central(s.cphys, s.len, g.L, g.M, l, s.p, out);
         if (WANT_WS && l >= 2 && l <= g.L - 1) {
-            const double wsp = fast_wave_speed(out, s.radius(l), g.gamma);
+            const double wsp = fast_wave_speed(out, r_l, ir_l, g.gamma);
             if (!isfinite(wsp)) nf = 1u;
             const unsigned long long kk = max_key(wsp, nf);
             ws_key = kk > ws_key ? kk : ws_key;
         }
     }
-    if (n < l_end) s.point(n, Un, q, r, Gz, gh, true, Acur, B);
+    if (n < l_end) s.point(rg, Un, q, r, Gz, gh, A, S);
+    r_l = r;
+    ir_l = q.ir;
     return true;
 }
 
@@ -139,29 +145,28 @@ __device__ __forceinline__ bool tma_band_run(TmaWarp &w, int l_begin, int l_end,
     w.jbase = j;
     for (int k = 0; k < kTmaStages; ++k) w.issue(j + k);
     bool ok;
-    double A0[9], A1[9], B[9], U[8], Gz[8], r;
+    double A[9], S[10], U[8], Gz[8], r, r_l = 1.0, ir_l = 1.0;
     FastPrim q;
+    RowGeo rg = s.row_geo(l_begin - 1);
     ok = w.take(j, U);
     if (ok) {
-        bool gh = s.eval(l_begin - 1, U, q, r, Gz);
+        bool gh = s.eval(l_begin - 1, rg, U, q, r, Gz);
         w.release(j);
         ++j;
-        s.point(l_begin - 1, U, q, r, Gz, gh, false, A0, B);  // A of the first cell row
+        fast_a(U, Gz, s.kz, A);  // A of the first cell row
+        rg = s.row_geo(l_begin);
         ok = w.take(j, U);
         if (ok) {
-            gh = s.eval(l_begin, U, q, r, Gz);
+            gh = s.eval(l_begin, rg, U, q, r, Gz);
             w.release(j);
             ++j;
-            s.point(l_begin, U, q, r, Gz, gh, true, A1, B);    // its B, and A of the next
+            s.point(rg, U, q, r, Gz, gh, A, S);  // S of the first cell row, A of the next
+            r_l = r;
+            ir_l = q.ir;
         }
     }
-    int l = l_begin;
-    // two rows per trip so the A buffers swap roles without copies
-    for (; ok && l + 1 < l_end; l += 2) {
-        ok = tma_row<WANT_WS>(w, l, l_end, j, A0, B, ws_key, nf);
-        if (ok) ok = tma_row<WANT_WS>(w, l + 1, l_end, j, A1, B, ws_key, nf);
-    }
-    if (ok && l < l_end) ok = tma_row<WANT_WS>(w, l, l_end, j, A0, B, ws_key, nf);
+    for (int l = l_begin; ok && l < l_end; ++l)
+        ok = tma_row<WANT_WS>(w, l, l_end, j, A, S, r_l, ir_l, ws_key, nf);
     if (!ok) {
         if (w.lane == 0) {
             const uint32_t end = w.jbase + (uint32_t)w.nrows;
