@@ -278,10 +278,11 @@ struct FastPrim {
     double ir;  // 1 / r of the point
 };
 
-MPD_HD FastPrim fast_prim(const double U[8], double r, double gm1) {
+// zero_iu: a ghost point (U = 0): 1/u_1 taken as 0, so that every value is 0.
+MPD_HD FastPrim fast_prim(const double U[8], double r, double gm1, bool zero_iu = false) {
     FastPrim q;
     const double ir = rcp_nr(r);
-    const double iu = rcp_nr(U[0]);
+    const double iu = zero_iu ? 0.0 : rcp_nr(U[0]);
     q.rho = U[0] * ir;
     q.vz = U[1] * iu;
     q.vr = U[2] * iu;

@@ -54,19 +54,14 @@ struct FastStrip {
 
     // Point row n, a cell row of this strip: its B (the r neighbours' shares
     // by warp shuffles, its own sources) folded with the row's A into S, then
-    // A replaced by the A this point row gives the cell row below it.  U must
-    // be zero on ghost points (the row staging guarantees it).  The shuffles
-    // sit outside every lane-dependent branch: all 32 lanes take part.
+    // A replaced by the A this point row gives the cell row below it.  On a
+    // ghost point U and q are zero, so its r fluxes are zero without a branch.
+    // The shuffles have all 32 lanes taking part.
     __device__ __forceinline__ void point(const RowGeo &rg, const double U[8], const FastPrim &q,
-                                          double r, const double Gz[8], bool gh, double A[9],
+                                          double r, const double Gz[8], double A[9],
                                           double S[10]) const {
         double Gr[8];
-        if (gh) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) Gr[k] = 0.0;
-        } else {
-            fast_gr(U, q, r, Gr);
-        }
+        fast_gr(U, q, r, Gr);
         // fast_rc + fast_b, each equation's two shuffles folded in as they arrive
         const double kr = dt * (0.5 / rg.dr);
         double B[9];
@@ -87,21 +82,16 @@ struct FastStrip {
         fast_a(U, Gz, kz, A);
     }
 
-    // Primitives and z fluxes of point row n (zeros on ghost points).
-    __device__ __forceinline__ bool eval(int n, const RowGeo &rg, const double U[8], FastPrim &q,
+    // Primitives and z fluxes of point row n.  Ghost points (U = 0 by the
+    // row staging) take 1/u_1 = 0 instead of a reciprocal of zero, which makes
+    // every primitive and flux exactly zero, as the reference's zero ghost
+    // values give, without a branch.
+    __device__ __forceinline__ void eval(int n, const RowGeo &rg, const double U[8], FastPrim &q,
                                          double &r, double Gz[8]) const {
         const bool gh = ghost(n);
-        if (gh) {
-            q = FastPrim{};
-            r = 1.0;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) Gz[k] = 0.0;
-        } else {
-            r = radius(rg);
-            q = fast_prim(U, r, gm1);
-            fast_gz(U, q, r, Gz);
-        }
-        return gh;
+        r = gh ? 1.0 : radius(rg);  // a ghost column past the wall may have no positive radius
+        q = fast_prim(U, r, gm1, gh);
+        fast_gz(U, q, r, Gz);
     }
 };
 

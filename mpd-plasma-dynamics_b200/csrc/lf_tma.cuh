@@ -95,38 +95,49 @@ struct TmaWarp {
     }
 };
 
-// Close cell row l (sums S) with point row n = l + 1 and fold that point row
-// in: S and A move on to row n.  r_l / ir_l: radius of row l and its
-// reciprocal (from the evaluation of point row l), replaced by row n's.
-template <bool WANT_WS>
-__device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, int l_end, uint32_t &j,
-                                        double A[9], double S[10], double &r_l, double &ir_l,
+// Close cell row l (sums S) with point row n = l + 1 and, unless it is the
+// band's last row (WITH_POINT false), fold that point row in: S and A move on
+// to row n.  r_l / ir_l: radius of row l and its reciprocal (from the
+// evaluation of point row l), replaced by row n's.
+//
+// After the stores the new cells' wave speed and point row n's shares are two
+// independent dependency chains in one branch-free stretch of code, so the
+// compiler interleaves them: every lane evaluates the wave speed (halo and
+// ghost lanes too, on whatever their values give) and only output lanes of
+// rows 2..L-1 feed it to the maximum.
+template <bool WANT_WS, bool WITH_POINT>
+__device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, uint32_t &j, double A[9],
+                                        double S[10], double &r_l, double &ir_l,
                                         unsigned long long &ws_key, unsigned int &nf) {
     const FastStrip &s = w.f;
+    const Geo &g = s.g;
     const int n = l + 1;
     const RowGeo rg = s.row_geo(n);  // issued before the wait, so the loads overlap it
     double Un[8];
     if (!w.take(j, Un)) return false;
     FastPrim q;
     double r, Gz[8], out[8];
-    const bool gh = s.eval(n, rg, Un, q, r, Gz);
+    s.eval(n, rg, Un, q, r, Gz);
     w.release(j);
     ++j;
     fast_finish(S, Un, Gz, s.kz, out);
     if (s.out_lane) {
-        const Geo &g = s.g;
         const size_t i = g.ix(l, s.p);
 #pragma unroll
         for (int k = 0; k < 8; ++k) s.u[(size_t)k * g.ps + i] = out[k];
         if (wants_central(g.L, g.M, l, s.p)) store_central(s.cphys, s.len, g.L, g.M, l, s.p, out);
-        if (WANT_WS && l >= 2 && l <= g.L - 1) {
-            const double wsp = fast_wave_speed(out, r_l, ir_l, g.gamma);
-            if (!isfinite(wsp)) nf = 1u;
-            const unsigned long long kk = max_key(wsp, nf);
+    }
+    if (WANT_WS) {
+        const double wsp = fast_wave_speed(out, r_l, ir_l, g.gamma);
+        const bool ws_lane = s.out_lane && l >= 2 && l <= g.L - 1;
+        unsigned int bad = 0u;
+        const unsigned long long kk = max_key(wsp, bad);
+        if (ws_lane) {
+            if (bad || !isfinite(wsp)) nf = 1u;
             ws_key = kk > ws_key ? kk : ws_key;
         }
     }
-    if (n < l_end) s.point(rg, Un, q, r, Gz, gh, A, S);
+    if (WITH_POINT) s.point(rg, Un, q, r, Gz, A, S);
     r_l = r;
     ir_l = q.ir;
     return true;
@@ -150,23 +161,25 @@ __device__ __forceinline__ bool tma_band_run(TmaWarp &w, int l_begin, int l_end,
     RowGeo rg = s.row_geo(l_begin - 1);
     ok = w.take(j, U);
     if (ok) {
-        bool gh = s.eval(l_begin - 1, rg, U, q, r, Gz);
+        s.eval(l_begin - 1, rg, U, q, r, Gz);
         w.release(j);
         ++j;
         fast_a(U, Gz, s.kz, A);  // A of the first cell row
         rg = s.row_geo(l_begin);
         ok = w.take(j, U);
         if (ok) {
-            gh = s.eval(l_begin, rg, U, q, r, Gz);
+            s.eval(l_begin, rg, U, q, r, Gz);
             w.release(j);
             ++j;
-            s.point(rg, U, q, r, Gz, gh, A, S);  // S of the first cell row, A of the next
+            s.point(rg, U, q, r, Gz, A, S);  // S of the first cell row, A of the next
             r_l = r;
             ir_l = q.ir;
         }
     }
-    for (int l = l_begin; ok && l < l_end; ++l)
-        ok = tma_row<WANT_WS>(w, l, l_end, j, A, S, r_l, ir_l, ws_key, nf);
+    int l = l_begin;
+    for (; ok && l < l_end - 1; ++l)
+        ok = tma_row<WANT_WS, true>(w, l, j, A, S, r_l, ir_l, ws_key, nf);
+    if (ok) ok = tma_row<WANT_WS, false>(w, l, j, A, S, r_l, ir_l, ws_key, nf);
     if (!ok) {
         if (w.lane == 0) {
             const uint32_t end = w.jbase + (uint32_t)w.nrows;
