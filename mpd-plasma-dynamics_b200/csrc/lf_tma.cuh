@@ -25,15 +25,18 @@
 namespace mpd {
 
 // Build-time tuning: resident blocks per SM the register budget is cut for,
-// and staged rows per warp.
+// staged rows per warp and warps per block.
 #ifndef MPD_TMA_MINB
 #define MPD_TMA_MINB 3
 #endif
 #ifndef MPD_TMA_STAGES
 #define MPD_TMA_STAGES 4
 #endif
+#ifndef MPD_TMA_WARPS
+#define MPD_TMA_WARPS 4
+#endif
 
-constexpr int kTmaWarps = 4;                  // warps per block
+constexpr int kTmaWarps = MPD_TMA_WARPS;      // warps per block
 constexpr int kTmaStages = MPD_TMA_STAGES;    // rows in flight per warp
 constexpr int kTmaRow = 8 * 32;               // doubles per staged row
 constexpr int kTmaRowBytes = kTmaRow * 8;     // 2048
@@ -78,13 +81,15 @@ struct TmaWarp {
         }
     }
 
-    // Staged row j into U (zeros on columns past M+1); false if the wait gave up.
+    // Staged row j into U; false if the wait gave up.  Columns past M+1 hold
+    // the zero ghost column M+2 or the tile's zero fill; their lanes write no
+    // cell and feed no output lane's sums either way.
     __device__ __forceinline__ bool take(uint32_t j, double U[8]) const {
         const uint32_t s = j % kTmaStages;
         const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar(s), (j / kTmaStages) & 1));
         const double *src = stage + s * kTmaRow + lane;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) U[k] = f.pvalid ? src[32 * k] : 0.0;
+        for (int k = 0; k < 8; ++k) U[k] = src[32 * k];
         return ok;
     }
 
@@ -225,25 +230,37 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
                   int nstrips, int nbands) {
     extern __shared__ __align__(128) unsigned char tma_smem_raw[];
     unsigned char *tma_smem = tma_smem_base(tma_smem_raw);
-    if (st->done) return;
-    const long long step = st->step;
     const int wib = threadIdx.x >> 5;
     const int task = (int)blockIdx.x * kTmaWarps + wib;
     const int strip = task % nstrips;
     const int band = task / nstrips;
+    int l_begin = 1, l_end = 1;
+    if (band < nbands) tma_band(g.L, nbands, band, l_begin, l_end);
+    const uint32_t bar0 =
+        smem_addr(tma_smem + kTmaWarps * kTmaStages * kTmaRowBytes) + 8u * wib * kTmaStages;
+    // While the previous kernel of the stream may still run: only this
+    // block's shared memory and the tensor maps, which no kernel writes.
+    if (l_begin < l_end && (threadIdx.x & 31) == 0) {
+        tmap_prefetch(&map0);
+        tmap_prefetch(&map1);
+        for (int k = 0; k < kTmaStages; ++k) mbar_init(bar0 + 8u * k, 1);
+        mbar_init_fence();
+    }
+    pdl_wait();
+    if (MPD_PDL_TRIG_INT == 1) pdl_trigger();
+    if (st->done) return;
+    const long long step = st->step;
 
     TmaWarp w;
     tma_warp_setup(w, g, strip, (step & 1) ? buf0 : buf1, st, cphys, len,
                    use_state_dt ? st->dt : dt_arg, (step & 1) ? &map1 : &map0);
     w.stage = reinterpret_cast<double *>(tma_smem) + wib * kTmaStages * kTmaRow;
-    w.bar0 = smem_addr(tma_smem + kTmaWarps * kTmaStages * kTmaRowBytes) + 8u * wib * kTmaStages;
+    w.bar0 = bar0;
 
     unsigned long long ws_key = 0ull;
     unsigned int nf = 0u;
-    int l_begin = 1, l_end = 1;
-    if (band < nbands) tma_band(g.L, nbands, band, l_begin, l_end);
     if (l_begin < l_end) {
-        w.init();
+        __syncwarp();
         uint32_t j = 0;
         if (!tma_band_run<WANT_WS>(w, l_begin, l_end, j, ws_key, nf) && w.lane == 0) {
             // a row never arrived: record the failure and stop the run
@@ -251,6 +268,7 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
             atomicExch(&st->done, 1);
         }
     }
+    if (MPD_PDL_TRIG_INT == 2) pdl_trigger();
     if (WANT_WS) {
         unsigned long long key[1] = {ws_key};
         unsigned long long *dst[1] = {&st->ws_acc};
@@ -289,18 +307,17 @@ inline cudaError_t plan_lf_tma(const Geo &g, int device, TmaPlan &plan) {
     return cudaSuccess;
 }
 
-inline void launch_lf_tma(const Geo &g, const TmaPlan &plan, const CUtensorMap &map0,
-                          const CUtensorMap &map1, double *buf0, double *buf1, DevState *st,
-                          double dt, int use_state_dt, bool want_ws, double *cphys, int len,
-                          cudaStream_t stream) {
+inline cudaError_t launch_lf_tma(const Geo &g, const TmaPlan &plan, const CUtensorMap &map0,
+                                 const CUtensorMap &map1, double *buf0, double *buf1,
+                                 DevState *st, double dt, int use_state_dt, bool want_ws,
+                                 double *cphys, int len, cudaStream_t stream) {
     if (want_ws)
-        lf_tma_kernel<true><<<plan.blocks, 32 * kTmaWarps, kTmaSmem, stream>>>(
-            g, map0, map1, buf0, buf1, st, dt, use_state_dt, cphys, len, plan.nstrips,
-            plan.nbands);
-    else
-        lf_tma_kernel<false><<<plan.blocks, 32 * kTmaWarps, kTmaSmem, stream>>>(
-            g, map0, map1, buf0, buf1, st, dt, use_state_dt, cphys, len, plan.nstrips,
-            plan.nbands);
+        return launch_pdl(lf_tma_kernel<true>, dim3(plan.blocks), dim3(32 * kTmaWarps), kTmaSmem,
+                          stream, g, map0, map1, buf0, buf1, st, dt, use_state_dt, cphys, len,
+                          plan.nstrips, plan.nbands);
+    return launch_pdl(lf_tma_kernel<false>, dim3(plan.blocks), dim3(32 * kTmaWarps), kTmaSmem,
+                      stream, g, map0, map1, buf0, buf1, st, dt, use_state_dt, cphys, len,
+                      plan.nstrips, plan.nbands);
 }
 
 }  // namespace mpd

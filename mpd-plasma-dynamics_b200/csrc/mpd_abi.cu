@@ -230,8 +230,8 @@ int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool
             mpd::lf_exact_kernel<false><<<grid, block, 0, s->stream>>>(
                 g, s->buf[0], s->buf[1], s->ic, s->st, dt, usd, s->cphys, s->len);
     } else {
-        mpd::launch_lf_tma(g, s->plan, s->tmap[0], s->tmap[1], s->buf[0], s->buf[1], s->st, dt,
-                           usd, want_ws, s->cphys, s->len, s->stream);
+        MPD_CK(mpd::launch_lf_tma(g, s->plan, s->tmap[0], s->tmap[1], s->buf[0], s->buf[1],
+                                  s->st, dt, usd, want_ws, s->cphys, s->len, s->stream));
     }
     MPD_CK(cudaGetLastError());
     return MPD_OK;
@@ -239,10 +239,11 @@ int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool
 
 int LaunchBoundary(mpd_solver *s, bool use_state_dt, double dt) {
     const int nring = mpd::ring_count(s->g);
-    mpd::bc_kernel<<<(nring + kBcBlock - 1) / kBcBlock, kBcBlock, 0, s->stream>>>(
-        s->g, s->buf[0], s->buf[1], s->ic, s->bc, s->st, dt, use_state_dt ? 1 : 0, s->cphys,
-        s->wall[0], s->wall[1], s->len, s->precision == MPD_PRECISION_FAST ? 1 : 0);
-    MPD_CK(cudaGetLastError());
+    MPD_CK(mpd::launch_pdl(mpd::bc_kernel, dim3((nring + kBcBlock - 1) / kBcBlock),
+                           dim3(kBcBlock), 0, s->stream, s->g, s->buf[0], s->buf[1],
+                           (const double *)s->ic, s->bc, s->st, dt, use_state_dt ? 1 : 0,
+                           (const double *)s->cphys, s->wall[0], s->wall[1], s->len,
+                           s->precision == MPD_PRECISION_FAST ? 1 : 0));
     return MPD_OK;
 }
 
