@@ -312,6 +312,13 @@ int mpd_nn_adam(float *p, const float *g, float *m, float *v, long long n, float
 int mpd_remap_snapshot(const double *d_src, int ni, int nj, int L_max, int M_max, double gamma,
                        double *d_out10, void *stream);
 
+/* ---- the fast path's reciprocal and square root ------------------------------ */
+/* New (no reference counterpart): d_rcp[i] = 1/x[i] and d_sqrt[i] = sqrt(x[i])
+ * for n device values, evaluated exactly as MPD_PRECISION_FAST evaluates them
+ * (hardware seed + polynomial correction), so a test can hold them to their
+ * error bound against correctly rounded results.  Asynchronous on `stream`. */
+int mpd_fast_math(const double *d_x, long long n, double *d_rcp, double *d_sqrt, void *stream);
+
 /* ---- host-side expression initial condition ---------------------------------- */
 /* ExpressionIC::Apply, src/ics/expression_ic.cpp:286-324, evaluated on the host
  * with the library's expression compiler.  exprs: 8 strings in the

@@ -142,6 +142,7 @@ SIGNATURES = [
                               C.c_float, C.c_int, _VP]),
     ("mpd_remap_snapshot", C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _VP,
                                      _VP]),
+    ("mpd_fast_math", C.c_int, [_VP, C.c_longlong, _VP, _VP, _VP]),
     ("mpd_expression_ic", C.c_int, [C.POINTER(Config), C.POINTER(Geometry), C.POINTER(C.c_char_p),
                                     C.c_int, C.POINTER(C.c_char_p), DP, DP]),
     ("mpd_eval_expression", C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), DP, DP]),

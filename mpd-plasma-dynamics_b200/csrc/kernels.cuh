@@ -205,15 +205,13 @@ __device__ __forceinline__ void ring_prefetch(const BcView &v, int l, int m) {
     }
 }
 
-// Boundary-ring slot i of one step (nothing for an idle slot): the cell's
-// final conserved values into v.u, and
-// the full reconstruction of the cell: its wave speed (want_ws) and, for the
-// wall columns, the "old" value the next step's faces read (wall lines wnext).
-__device__ __forceinline__ void ring_cell_update(const BcView &v, int i, double *wnext,
-                                                 bool want_ws, CellStats &cs) {
+// Boundary-ring cell (l, m) of one step: its final conserved values into v.u,
+// and the full reconstruction of the cell: its wave speed (want_ws) and, for
+// the wall columns, the "old" value the next step's faces read (wall lines
+// wnext).
+__device__ __forceinline__ void ring_cell_at(const BcView &v, int l, int m, double *wnext,
+                                             bool want_ws, CellStats &cs) {
     const Geo &g = v.g;
-    int l, m;
-    if (!ring_cell(g, i, l, m)) return;
     ring_prefetch(v, l, m);
     double uf[8];
     bc_ring_final(v, l, m, uf);
@@ -228,6 +226,94 @@ __device__ __forceinline__ void ring_cell_update(const BcView &v, int i, double 
             cs.add_ws(v.fast ? fast_wave_speed(uf, r, rcp_nr(r), g.gamma) : wave_speed(q, g.gamma));
         if (wall) store_line_phys(wnext, v.len, m == 1 ? 0 : 1, l, q);
     }
+}
+
+// Boundary-ring slot i of one step (nothing for an idle slot).
+__device__ __forceinline__ void ring_cell_update(const BcView &v, int i, double *wnext,
+                                                 bool want_ws, CellStats &cs) {
+    int l, m;
+    if (ring_cell(v.g, i, l, m)) ring_cell_at(v, l, m, wnext, want_ws, cs);
+}
+
+// The boundary inputs of one step: views of the state, the central and wall
+// lines and the face table.
+__device__ __forceinline__ BcView make_bc_view(const Geo &g, const double *u0, double *u,
+                                               const double *ic, const double *cphys,
+                                               const double *wphys, int len, bool first, int fast,
+                                               double dt, const BcTable &bc) {
+    BcView v;
+    v.g = g;
+    v.u0 = u0;
+    v.u = u;
+    v.ic = ic;
+    v.cphys = cphys;
+    v.wphys = wphys;
+    v.len = len;
+    v.first = first ? 1 : 0;
+    v.fast = fast;
+    v.dt = dt;
+    v.bc = bc;
+    return v;
+}
+
+// True in thread 0 of the last block of the grid to get here, after every
+// block's writes (state, lines, reduction atomics) are visible to it.  Every
+// thread of every block calls it.
+__device__ __forceinline__ bool last_block_arrived(DevState *st) {
+    __shared__ int is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(&st->arrive, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!is_last || threadIdx.x != 0) return false;
+    __threadfence();
+    return true;
+}
+
+// End of step `step` (dt the step used), run by one thread once every cell's
+// reductions are in: wave speed and non-finite flag, t and step, and in run
+// mode the next dt and the stop flags; then the accumulators are cleared.
+__device__ __forceinline__ void step_controller(const Geo &g, DevState *st, long long step,
+                                                double dt, int flags) {
+    // All reads first, through L2 and independent of each other, so the
+    // controller costs one memory round trip instead of one per field.
+    const unsigned long long ws_bits = __ldcg(&st->ws_acc);
+    const unsigned int nf_acc = __ldcg(&st->nf_acc);
+    const double t0 = __ldcg(&st->t);
+    const int nonfinite0 = __ldcg(&st->nonfinite);
+    const int run_mode = __ldcg(&st->run_mode);
+    const int adaptive = __ldcg(&st->adaptive);
+    const double cfl = __ldcg(&st->cfl), growth = __ldcg(&st->growth);
+    const double dt_min = __ldcg(&st->dt_min), dt_max = __ldcg(&st->dt_max);
+    const double T = __ldcg(&st->T);
+    const long long max_steps = __ldcg(&st->max_steps);
+    const double conv_thr = __ldcg(&st->conv_thr);
+    const int check_freq = __ldcg(&st->check_freq);
+
+    const double ws = (flags & kFlagWs) ? __longlong_as_double((long long)ws_bits) : 0.0;
+    if (flags & kFlagWs) st->last_ws = ws;
+    st->ws_valid = (flags & kFlagWs) ? 1 : 0;
+    const int nonfinite = (nonfinite0 || nf_acc || !isfinite(ws)) ? 1 : 0;
+    st->nonfinite = nonfinite;
+    const double t = t0 + dt;
+    const long long nstep = step + 1;
+    st->t = t;
+    st->dt_used = dt;
+    st->step = nstep;
+    st->resid_valid = 0;  // the residual of this step is evaluated on request
+    if (run_mode) {
+        double dtn = dt;
+        if (adaptive) dtn = compute_dt_from_speed(ws, g.dz, g.dy, cfl, growth, dt_min, dt_max, dt);
+        const int done = (nonfinite || !(t < T) || nstep >= max_steps) ? 1 : 0;
+        if (t + dtn > T) dtn = T - t;
+        st->dt = dtn;
+        st->check_due = (conv_thr > 0.0 && check_freq > 0 && nstep % check_freq == 0) ? 1 : 0;
+        st->done = done;
+    }
+    st->ws_acc = 0ull;
+    st->nf_acc = 0u;
+    __threadfence();
+    st->arrive = 0u;
 }
 
 // Exact interior update (Solver::ComputeCentralUpdate + the implicit
@@ -279,8 +365,19 @@ __global__ void __launch_bounds__(256) lf_exact_kernel(Geo g, double *buf0, doub
 }
 
 // Boundary faces, one thread per boundary-ring cell, plus the end-of-step
-// controller in the last block to finish.
-__global__ void __launch_bounds__(64) bc_kernel(Geo g, double *buf0, double *buf1,
+// controller in the last block to finish.  A few thousand threads on a
+// dependent chain: registers are not what limits it, spills would lengthen
+// the chain, so the register budget is lifted (MPD_BC_MAXNREG 0: the
+// compiler's default for 64-thread blocks).
+#ifndef MPD_BC_MAXNREG
+#define MPD_BC_MAXNREG 0
+#endif
+#if MPD_BC_MAXNREG
+#define MPD_BC_BOUNDS __maxnreg__(MPD_BC_MAXNREG)
+#else
+#define MPD_BC_BOUNDS __launch_bounds__(64)
+#endif
+__global__ void MPD_BC_BOUNDS bc_kernel(Geo g, double *buf0, double *buf1,
                                                  const double *__restrict__ ic, BcTable bc,
                                                  DevState *st, double dt_arg, int use_state_dt,
                                                  const double *cphys, double *wall0, double *wall1,
@@ -293,18 +390,8 @@ __global__ void __launch_bounds__(64) bc_kernel(Geo g, double *buf0, double *buf
     double *u = (step & 1) ? buf0 : buf1;
     const double dt = use_state_dt ? st->dt : dt_arg;
     const int flags = step_flags(st);
-    BcView v;
-    v.g = g;
-    v.u0 = u0;
-    v.u = u;
-    v.ic = ic;
-    v.cphys = cphys;
-    v.wphys = (step & 1) ? wall1 : wall0;
-    v.len = len;
-    v.first = step == 0;
-    v.fast = fast;
-    v.dt = dt;
-    v.bc = bc;
+    const BcView v = make_bc_view(g, u0, u, ic, cphys, (step & 1) ? wall1 : wall0, len,
+                                  step == 0, fast, dt, bc);
     double *wnext = (step & 1) ? wall0 : wall1;
     CellStats cs;
     cs.init();
@@ -312,54 +399,7 @@ __global__ void __launch_bounds__(64) bc_kernel(Geo g, double *buf0, double *buf
     if (i < ring_count(g)) ring_cell_update(v, i, wnext, (flags & kFlagWs) != 0, cs);
     if (flags) cs.flush(st);
     if (MPD_PDL_TRIG_BC == 2) pdl_trigger();
-
-    // ---- last block: finalise the step -------------------------------------
-    __shared__ int is_last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) is_last = atomicAdd(&st->arrive, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!is_last || threadIdx.x != 0) return;
-    __threadfence();
-    // All reads first, through L2 and independent of each other, so the
-    // controller costs one memory round trip instead of one per field.
-    const unsigned long long ws_bits = __ldcg(&st->ws_acc);
-    const unsigned int nf_acc = __ldcg(&st->nf_acc);
-    const double t0 = __ldcg(&st->t);
-    const int nonfinite0 = __ldcg(&st->nonfinite);
-    const int run_mode = __ldcg(&st->run_mode);
-    const int adaptive = __ldcg(&st->adaptive);
-    const double cfl = __ldcg(&st->cfl), growth = __ldcg(&st->growth);
-    const double dt_min = __ldcg(&st->dt_min), dt_max = __ldcg(&st->dt_max);
-    const double T = __ldcg(&st->T);
-    const long long max_steps = __ldcg(&st->max_steps);
-    const double conv_thr = __ldcg(&st->conv_thr);
-    const int check_freq = __ldcg(&st->check_freq);
-
-    const double ws = (flags & kFlagWs) ? __longlong_as_double((long long)ws_bits) : 0.0;
-    if (flags & kFlagWs) st->last_ws = ws;
-    st->ws_valid = (flags & kFlagWs) ? 1 : 0;
-    const int nonfinite = (nonfinite0 || nf_acc || !isfinite(ws)) ? 1 : 0;
-    st->nonfinite = nonfinite;
-    const double t = t0 + dt;
-    const long long nstep = step + 1;
-    st->t = t;
-    st->dt_used = dt;
-    st->step = nstep;
-    st->resid_valid = 0;  // the residual of this step is evaluated on request
-    if (run_mode) {
-        double dtn = dt;
-        if (adaptive) dtn = compute_dt_from_speed(ws, g.dz, g.dy, cfl, growth, dt_min, dt_max, dt);
-        const int done = (nonfinite || !(t < T) || nstep >= max_steps) ? 1 : 0;
-        if (t + dtn > T) dtn = T - t;
-        st->dt = dtn;
-        st->check_due = (conv_thr > 0.0 && check_freq > 0 && nstep % check_freq == 0) ? 1 : 0;
-        st->done = done;
-    }
-    st->ws_acc = 0ull;
-    st->nf_acc = 0u;
-    __threadfence();
-    st->arrive = 0u;
+    if (last_block_arrived(st)) step_controller(g, st, step, dt, flags);
 }
 
 // L-inf residual of the step that just finished (new; the reference has only

@@ -234,11 +234,12 @@ MPD_HD void lf_cell_exact(const double U[5][8], const Phys Q[5], const double R[
 // Newton iteration from a single-precision seed.
 // ---------------------------------------------------------------------------
 
-// 1/x: a seed of at least 16 correct bits, then two Newton-Raphson steps
-// y <- y + y (1 - x y), each squaring the relative error (2^-32, then below
-// double rounding).  On the device the seed is the hardware's double-precision
-// reciprocal approximation (rcp.approx.ftz.f64, from the upper word of x: no
-// conversions, any normal double); on the host a single-precision reciprocal.
+// 1/x from a seed y0 = (1 - e) / x: y0 (1 + e + e^2) = (1 - e^3) / x, three
+// dependent FMAs.  On the device the seed is the hardware's double-precision
+// reciprocal approximation (rcp.approx.ftz.f64: no conversions, any normal
+// double), measured on a B200 at |e| <= 2^-19.9 over 2^28 inputs across
+// exponents -60..60, so e^3 <= 2^-59 is below double rounding; on the host a
+// single-precision reciprocal (|e| <= 2^-24).
 MPD_HD double rcp_nr(double x) {
 #ifdef __CUDA_ARCH__
     double y;
@@ -246,17 +247,15 @@ MPD_HD double rcp_nr(double x) {
 #else
     double y = (double)(1.0f / (float)x);
 #endif
-    double e = fma(-x, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-x, y, 1.0);
-    return fma(y, e, y);
+    const double e = fma(-x, y, 1.0);
+    return fma(y, fma(e, e, e), y);
 }
 
-// sqrt(a) (0 -> 0, a < 0 -> NaN): a 1/sqrt seed y0 of at least 16 correct
-// bits, one Newton step y <- y (3 - a y^2) / 2 (relative error 1.5 e0^2 <=
-// 2^-31), then s = a y and one Heron correction s <- s + y (a - s^2) / 2, which
-// leaves a relative error of e^2 / 2 (below 2^-62).  Device seed:
-// rsqrt.approx.ftz.f64; host seed: single precision.
+// sqrt(a) (0 -> 0, a < 0 -> NaN) from a 1/sqrt seed y0: with t = a y0 and
+// d = 1 - t y0, sqrt(a) = t (1 - d)^(-1/2) = t (1 + d/2 + 3 d^2 / 8 + ...); the
+// two terms kept leave 5 d^3 / 16.  Device seed: rsqrt.approx.ftz.f64, measured
+// at 2^-20.0 relative (d <= 2^-19, so 5 d^3 / 16 <= 2^-58); host seed: single
+// precision.
 MPD_HD double sqrt_nr(double a) {
 #ifdef __CUDA_ARCH__
     double y;
@@ -264,11 +263,9 @@ MPD_HD double sqrt_nr(double a) {
 #else
     double y = (double)(1.0f / sqrtf((float)a));
 #endif
-    const double ha = 0.5 * a;
-    y = y * fma(-ha * y, y, 1.5);
-    const double s = a * y;
-    const double r = fma(-s, s, a);
-    const double out = fma(0.5 * y, r, s);
+    const double t = a * y;
+    const double d = fma(-t, y, 1.0);
+    const double out = fma(t, d * fma(d, 0.375, 0.5), t);
     return a > 0.0 ? out : (a == 0.0 ? 0.0 : NAN);
 }
 
@@ -715,9 +712,16 @@ MPD_HD double bc_binop(int op, double a, double b) {
 // 286-292 resolve, 311-360 / 393-446 expression path): writes the 8 new
 // primitives of cell (l, m) given its neighbour's primitives and the values
 // to keep (AxisLF fields keep the cell's current value).
+#ifndef MPD_SEG_UNROLL
+#define MPD_SEG_UNROLL 0
+#endif
 MPD_HD void eval_segment(const BcView &v, const SegDesc &d, int l, int m, int ln, int mn,
                          const Prim &nb, const Prim &keep, Prim &out) {
+#if MPD_SEG_UNROLL
+#pragma unroll
+#else
 #pragma unroll 1
+#endif
     for (int j = 0; j < 8; ++j) {
         double val;
         switch (d.type[j]) {

@@ -25,7 +25,7 @@
 namespace mpd {
 
 // Build-time tuning: resident blocks per SM the register budget is cut for,
-// staged rows per warp and warps per block.
+// staged rows per warp, warps per block and the fewest rows a band gets.
 #ifndef MPD_TMA_MINB
 #define MPD_TMA_MINB 3
 #endif
@@ -34,6 +34,9 @@ namespace mpd {
 #endif
 #ifndef MPD_TMA_WARPS
 #define MPD_TMA_WARPS 4
+#endif
+#ifndef MPD_TMA_MIN_BAND
+#define MPD_TMA_MIN_BAND 4
 #endif
 
 constexpr int kTmaWarps = MPD_TMA_WARPS;      // warps per block
@@ -298,7 +301,7 @@ inline cudaError_t plan_lf_tma(const Geo &g, int device, TmaPlan &plan) {
     const int warps = sms * per_sm * kTmaWarps;
     plan.nstrips = (g.M + kFastCells - 1) / kFastCells;
     int nb = warps / plan.nstrips;
-    const int min_band = 4;  // rows; each band re-reads two rows above its first
+    const int min_band = MPD_TMA_MIN_BAND;  // rows; each band re-reads two rows above its first
     if (nb > g.L / min_band) nb = g.L / min_band;
     if (nb < 1) nb = 1;
     plan.nbands = nb;

@@ -215,8 +215,8 @@ int UploadPhysical(mpd_solver *s, const double *phys10) {
 
 // One time step: interior kernel, boundary kernel (+ controller), in run mode
 // the guarded relative-L2 convergence check and, every residual_every steps,
-// the L-inf residual.  want_ws: fuse the maximum wave speed (adaptive dt and
-// the per-call ComputeDt need it).
+// the L-inf residual.  want_ws: fuse the maximum
+// wave speed (adaptive dt and the per-call ComputeDt need it).
 int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool want_ws) {
     const mpd::Geo &g = s->g;
     const int usd = use_state_dt ? 1 : 0;
@@ -319,9 +319,28 @@ int BuildGraph(mpd_solver *s, int steps, bool with_check, bool want_ws, int resi
     return MPD_OK;
 }
 
+__global__ void fast_math_kernel(const double *x, long long n, double *rcp, double *sqr) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        rcp[i] = mpd::rcp_nr(x[i]);
+        sqr[i] = mpd::sqrt_nr(x[i]);
+    }
+}
+
 }  // namespace
 
 extern "C" {
+
+int mpd_fast_math(const double *d_x, long long n, double *d_rcp, double *d_sqrt, void *stream) {
+    if (!d_x || !d_rcp || !d_sqrt || n < 0) return Fail(MPD_ERR_INVALID, "mpd_fast_math: bad arguments");
+    if (n == 0) return MPD_OK;
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    fast_math_kernel<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(d_x, n, d_rcp,
+                                                                                     d_sqrt);
+    MPD_CK(cudaGetLastError());
+    return MPD_OK;
+}
 
 const char *mpd_last_error(void) { return mpd::g_last_error.c_str(); }
 
