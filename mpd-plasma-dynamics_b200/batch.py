@@ -156,8 +156,8 @@ class Autotuner:
         out = {}
         s.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=2)   # first step, warm
         for blocks in self.candidates:
-            if blocks * 4 > 4 * max(1, (cfg.M_max + 29) // 30) * max(1, cfg.L_max // 4):
-                break   # more warps than interior tasks
+            if blocks * 4 > max(1, (cfg.M_max + 29) // 30) * max(1, cfg.L_max):
+                break   # more warps than interior tasks (strips x one-row bands)
             plan = BatchPlan([blocks], [0])
             b.run(plan, max_steps=10, residual_every=0)
             r = b.run(plan, max_steps=self.steps, residual_every=0)

@@ -368,9 +368,10 @@ __global__ void __launch_bounds__(256) lf_exact_kernel(Geo g, double *buf0, doub
 // controller in the last block to finish.  A few thousand threads on a
 // dependent chain: registers are not what limits it, spills would lengthen
 // the chain, so the register budget is lifted (MPD_BC_MAXNREG 0: the
-// compiler's default for 64-thread blocks).
+// compiler's default for 64-thread blocks, 128 registers with spills; 255:
+// ~214, no spills, 100 x 40 step 18.2 -> 17.4 us on a B200).
 #ifndef MPD_BC_MAXNREG
-#define MPD_BC_MAXNREG 0
+#define MPD_BC_MAXNREG 255
 #endif
 #if MPD_BC_MAXNREG
 #define MPD_BC_BOUNDS __maxnreg__(MPD_BC_MAXNREG)

@@ -471,12 +471,12 @@ inline cudaError_t persist_blocks_per_sm(int &per_sm) {
 }
 
 // Interior tasks of a solve run by a team of `blocks` blocks: strips of 30
-// columns x bands of at least 4 rows, about one task per warp.
+// columns x bands of at least MPD_TMA_MIN_BAND rows, about one task per warp.
 inline void persist_tasks(const Geo &g, int blocks, int &nstrips, int &nbands) {
     const int warps = blocks * kTmaWarps;
     nstrips = (g.M + kFastCells - 1) / kFastCells;
     int nb = warps / nstrips;
-    if (nb > g.L / 4) nb = g.L / 4;
+    if (nb > g.L / MPD_TMA_MIN_BAND) nb = g.L / MPD_TMA_MIN_BAND;
     if (nb < 1) nb = 1;
     nbands = nb;
 }

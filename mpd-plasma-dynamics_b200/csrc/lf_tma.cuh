@@ -26,6 +26,9 @@ namespace mpd {
 
 // Build-time tuning: resident blocks per SM the register budget is cut for,
 // staged rows per warp, warps per block and the fewest rows a band gets.
+// A small grid has more warps than (strip, row) pairs: one-row bands then
+// give the shortest chain per warp (measured on a B200: 100 x 40 step
+// 18.2 -> 15.4 us, 400 x 160 18.1 -> 16.7 us; large grids unaffected).
 #ifndef MPD_TMA_MINB
 #define MPD_TMA_MINB 3
 #endif
@@ -36,7 +39,7 @@ namespace mpd {
 #define MPD_TMA_WARPS 4
 #endif
 #ifndef MPD_TMA_MIN_BAND
-#define MPD_TMA_MIN_BAND 4
+#define MPD_TMA_MIN_BAND 1
 #endif
 
 constexpr int kTmaWarps = MPD_TMA_WARPS;      // warps per block
