@@ -373,6 +373,10 @@ __global__ void __launch_bounds__(256) lf_exact_kernel(Geo g, double *buf0, doub
 #ifndef MPD_BC_MAXNREG
 #define MPD_BC_MAXNREG 255
 #endif
+#ifndef MPD_BC_SMEM_SEG
+#define MPD_BC_SMEM_SEG 1
+#endif
+static_assert(sizeof(SegDesc) % 16 == 0, "segment descriptors are copied as 16-byte words");
 #if MPD_BC_MAXNREG
 #define MPD_BC_BOUNDS __maxnreg__(MPD_BC_MAXNREG)
 #else
@@ -383,6 +387,20 @@ __global__ void MPD_BC_BOUNDS bc_kernel(Geo g, double *buf0, double *buf1,
                                                  DevState *st, double dt_arg, int use_state_dt,
                                                  const double *cphys, double *wall0, double *wall1,
                                                  int len, int fast) {
+#if MPD_BC_SMEM_SEG
+    // The face segments into shared memory (dynamic, nseg_total of them):
+    // every ring cell walks them in its dependent chain.  No kernel writes
+    // them, so this runs before the previous kernel of the stream is waited for.
+    extern __shared__ __align__(16) unsigned char bc_smem_raw[];
+    {
+        const int4 *src = reinterpret_cast<const int4 *>(bc.seg);
+        int4 *dst = reinterpret_cast<int4 *>(bc_smem_raw);
+        const int n = bc.nseg_total * (int)(sizeof(SegDesc) / sizeof(int4));
+        for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
+        __syncthreads();
+        bc.seg = reinterpret_cast<const SegDesc *>(bc_smem_raw);
+    }
+#endif
     pdl_wait();
     if (MPD_PDL_TRIG_BC == 1) pdl_trigger();
     if (st->done) return;

@@ -376,6 +376,24 @@ MPD_HD void fast_finish(const double S[10], const double Un[8], const double Gzn
 // with reciprocals and Newton square roots:
 //   |v|^2 = (u_2^2 + u_3^2) / u_1^2,  c_s^2 = gamma (gamma - 1) u_5 / u_1,
 //   c_a^2 = (H_z^2 + H_r^2 + H_phi^2) r / u_1   (u_1 = rho r, u_5 = rho e r).
+// The wave speed's square roots, without special cases: the argument is
+// nudged by 1e-300, which leaves every argument above 1e-284 unchanged (it is
+// below half an ulp), turns 0 into a root of 1e-150 that vanishes in the
+// sum, and keeps a negative argument's NaN (an unphysical state, caught by
+// the non-finite check).
+MPD_HD double sqrt_speed(double a) {
+    a += 1e-300;
+#ifdef __CUDA_ARCH__
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+#else
+    double y = (double)(1.0f / sqrtf((float)a));
+#endif
+    const double t = a * y;
+    const double d = fma(-t, y, 1.0);
+    return fma(t, d * fma(d, 0.375, 0.5), t);
+}
+
 MPD_HD double fast_wave_speed(const double u[8], double r, double ir, double gamma) {
     const double iu = rcp_nr(u[0]);
     const double vz = u[1] * iu, vr = u[2] * iu;
@@ -383,7 +401,7 @@ MPD_HD double fast_wave_speed(const double u[8], double r, double ir, double gam
     const double cs2 = gamma * (gamma - 1.0) * u[4] * iu;
     const double ca2 = fma(Hz, Hz, fma(Hr, Hr, Hphi * Hphi)) * (r * iu);
     const double v2 = fma(vz, vz, vr * vr);
-    return sqrt_nr(v2) + sqrt_nr(cs2) + sqrt_nr(ca2);
+    return sqrt_speed(v2) + sqrt_speed(cs2) + sqrt_speed(ca2);
 }
 
 // ---------------------------------------------------------------------------

@@ -139,14 +139,13 @@ __device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, uint32_t &j, do
         if (wants_central(g.L, g.M, l, s.p)) store_central(s.cphys, s.len, g.L, g.M, l, s.p, out);
     }
     if (WANT_WS) {
+        // The wave speed is positive or NaN / inf, so its bits order like its
+        // value with NaN and inf above every finite speed: a non-finite cell
+        // wins the maximum and the controller flags the step.
         const double wsp = fast_wave_speed(out, r_l, ir_l, g.gamma);
         const bool ws_lane = s.out_lane && l >= 2 && l <= g.L - 1;
-        unsigned int bad = 0u;
-        const unsigned long long kk = max_key(wsp, bad);
-        if (ws_lane) {
-            if (bad || !isfinite(wsp)) nf = 1u;
-            ws_key = kk > ws_key ? kk : ws_key;
-        }
+        const unsigned long long kk = ws_lane ? (unsigned long long)__double_as_longlong(wsp) : 0ull;
+        ws_key = kk > ws_key ? kk : ws_key;
     }
     if (WITH_POINT) s.point(rg, Un, q, r, Gz, A, S);
     r_l = r;

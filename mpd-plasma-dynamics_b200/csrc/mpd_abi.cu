@@ -239,8 +239,9 @@ int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool
 
 int LaunchBoundary(mpd_solver *s, bool use_state_dt, double dt) {
     const int nring = mpd::ring_count(s->g);
+    const size_t smem = MPD_BC_SMEM_SEG ? s->bc.nseg_total * sizeof(mpd::SegDesc) : 0;
     MPD_CK(mpd::launch_pdl(mpd::bc_kernel, dim3((nring + kBcBlock - 1) / kBcBlock),
-                           dim3(kBcBlock), 0, s->stream, s->g, s->buf[0], s->buf[1],
+                           dim3(kBcBlock), smem, s->stream, s->g, s->buf[0], s->buf[1],
                            (const double *)s->ic, s->bc, s->st, dt, use_state_dt ? 1 : 0,
                            (const double *)s->cphys, s->wall[0], s->wall[1], s->len,
                            s->precision == MPD_PRECISION_FAST ? 1 : 0));

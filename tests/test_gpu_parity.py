@@ -296,3 +296,24 @@ def test_vtk_restart_remap_matches_oracle(pkg, tmp_path):
     r = s2.run(T=1e300, dt=0.0, adaptive=True, max_steps=50)
     assert r.steps == 50 and r.status == 0
     s2.close()
+
+
+@pytest.mark.parametrize("precision,engine", [("fast", "graph"), ("fast", "persistent"),
+                                              ("exact", "graph")])
+def test_blowup_is_flagged_nonfinite(pkg, precision, engine):
+    """A CFL number far above 1 makes the scheme blow up; the step whose new
+    state has the first Inf/NaN wave speed (overflow, or a negative energy
+    before any conserved value overflows) stops the run with
+    MPD_ERR_NONFINITE, the same step in every engine."""
+    case = cases.channel_case(L=48, M=20, cfl=40.0)
+    cfg = case.cfg
+    s = pkg.GpuSolver(cfg, case.grid, case.phys, precision=precision)
+    res = s.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=5000, engine=engine)
+    assert res.status == pkg._native.MPD_ERR_NONFINITE
+    assert 1 < res.steps < 5000
+    s.close()
+    if precision == "fast" and engine == "persistent":
+        g = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+        rg = g.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=5000, engine="graph")
+        assert rg.steps == res.steps
+        g.close()
