@@ -432,40 +432,70 @@ def run_surrogate(args):
             "vs_baseline": None, "gemm_tflops": flops / (ms * 1e-3) / 1e12}
 
 
-def run_batch(args):
-    """The batched sweep: n solves drawn from the sweep box (uneven grids),
-    autotuned teams, one persistent cooperative launch, cold start."""
+def run_batch(args, rank=0, world=1, local_rank=0):
+    """The batched sweep: n solves per GPU drawn from the sweep box (uneven
+    grids), autotuned teams, one persistent cooperative launch per GPU, cold
+    start.  With N GPUs (one process each) the N x n draws shard by solve,
+    balanced by estimated cost; nothing crosses GPUs while solving, the
+    results are gathered on rank 0 and the time is the slowest rank's."""
     import numpy as np
+    import torch
     import __graft_entry__
     pkg = __graft_entry__.load_package()
-    params = [pkg.workloads.sweep_params(i) for i in range(args.n_solves)]
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local_rank))
+    n_total = args.n_solves * world
+    params = [pkg.workloads.sweep_params(i) for i in range(n_total)]
     cfgs = [p.config() for p in params]
-    solvers = [pkg.build_case(c, precision="fast") for c in cfgs]
-    batch = pkg.BatchSolver(solvers)
-    tuner = pkg.Autotuner(batch.capacity, steps=100)
-    plan = tuner.plan(cfgs, max_steps=args.max_steps)
-    res = batch.run(plan, max_steps=args.max_steps, residual_tol=1e-8, residual_every=50)
-    cells = sum(c.L_max * (c.M_max + 1) * r.steps for c, r in zip(cfgs, res.runs))
-    line = {
-        "metric": "batched steady solves: solves/s", "unit": "solves/s", "n_gpus": 1,
-        "value": args.n_solves / (res.device_ms * 1e-3), "higher_is_better": True,
-        "dtype": "f64", "data": "synthetic (sweep-box draws, numpy default_rng(i))",
+    info = {}
+
+    def run_share(idx):
+        sub = [cfgs[i] for i in idx]
+        solvers = [pkg.build_case(c, precision="fast") for c in sub]
+        batch = pkg.BatchSolver(solvers)
+        tuner = pkg.Autotuner(batch.capacity, steps=100)
+        plan = tuner.plan(sub, max_steps=args.max_steps)
+        res = batch.run(plan, max_steps=args.max_steps, residual_tol=1e-8, residual_every=50)
+        info["plan"], info["table"] = plan, tuner.table
+        batch.close()
+        for s in solvers:
+            s.close()
+        return res.runs, res.solve_ms, res.device_ms
+
+    if world > 1:
+        costs = [pkg.sharding.solve_cost(c, args.max_steps) for c in cfgs]
+        merged = pkg.sharding.run_sharded(costs, run_share)
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank != 0:
+            return None
+        runs, solve_ms, device_ms = merged.runs, merged.solve_ms, merged.device_ms
+    else:
+        runs, solve_ms, device_ms = run_share(list(range(n_total)))
+    plan = info["plan"]
+    converged = int(sum(bool(r.converged) for r in runs))
+    cells = sum(c.L_max * (c.M_max + 1) * r.steps for c, r in zip(cfgs, runs))
+    return {
+        "metric": "batched steady solves: solves/s", "unit": "solves/s", "n_gpus": world,
+        "value": n_total / (device_ms * 1e-3), "higher_is_better": True,
+        "scaling": "weak", "dtype": "f64", "data": "synthetic (sweep-box draws, numpy default_rng(i))",
         "config": {"workload": "batched sweep, grids {100x40,200x80,400x160,800x320}",
-                   "n_solves": args.n_solves, "max_steps": args.max_steps,
-                   "teams": len(plan.team_blocks), "blocks": plan.blocks},
+                   "n_solves": n_total, "n_solves_per_gpu": args.n_solves,
+                   "max_steps": args.max_steps,
+                   "teams_rank0": len(plan.team_blocks), "blocks_rank0": plan.blocks,
+                   "sharding": "by solve, cost-balanced" if world > 1 else "none"},
         "vs_baseline": None,
-        "cell_updates_per_s": cells / (res.device_ms * 1e-3),
-        "converged": int(res.converged.sum()),
-        "p50_solve_ms": float(np.percentile(res.solve_ms, 50)),
-        "p99_solve_ms": float(np.percentile(res.solve_ms, 99)),
-        "device_ms": res.device_ms,
-        "plan": {"team_blocks": plan.team_blocks},
-        "autotune_us_per_step": {f"{k[0]}x{k[1]}": v for k, v in tuner.table.items()},
+        "cell_updates_per_s": cells / (device_ms * 1e-3),
+        "converged": converged,
+        "p50_solve_ms": float(np.percentile(solve_ms, 50)),
+        "p99_solve_ms": float(np.percentile(solve_ms, 99)),
+        "device_ms": device_ms,
+        "plan_rank0": {"team_blocks": plan.team_blocks},
+        "autotune_us_per_step": {f"{k[0]}x{k[1]}": v for k, v in info["table"].items()},
     }
-    batch.close()
-    for s in solvers:
-        s.close()
-    return line
 
 
 def run_profile(args):
@@ -523,10 +553,15 @@ def main():
     if args.profile:
         run_profile(args)
         return
+    if args.workload == "batch":
+        line = run_batch(args, rank, world, local_rank)
+        if line is not None:
+            print(json.dumps(line))
+        return
     if args.workload != "plain":
         if rank == 0:
-            runner = {"warmstart": run_warmstart, "batch": run_batch,
-                      "surrogate": run_surrogate, "serve": run_serve}[args.workload]
+            runner = {"warmstart": run_warmstart, "surrogate": run_surrogate,
+                      "serve": run_serve}[args.workload]
             line = runner(args)
             print(json.dumps(line))
         return

@@ -5,9 +5,10 @@ The compute path is the CUDA library ``libmpd_b200.so`` behind the C ABI of
 ``include/mpd_b200.h``; this package is its Python host side: configuration
 (``config``), geometry plugins and grid profiles (``geometry``), initial
 conditions (``ic``), the solver handle (``solver``), batched solves and their
-autotuner (``batch``).
+autotuner (``batch``), batched solves sharded over the GPUs of a node
+(``sharding``).
 """
-from . import _native, io, nn, serve, surrogate, warmstart, workloads
+from . import _native, io, nn, serve, sharding, surrogate, warmstart, workloads
 from .config import BCSegmentConfig, ConfigError, FieldCond, SimConfig, segment
 from .geometry import GeometryRegistry, Grid, IGeometry, register_all_geometries
 from .ic import ArrayIC, ExpressionIC, IInitialCondition
