@@ -59,6 +59,15 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
 #endif
 }
 
+// What the per-call host path (mpd_compute_dt after mpd_advance) needs of
+// the controller, written by it into mapped pinned host memory each step, so
+// the host reads it after an event instead of copying the whole state back.
+struct HostMirror {
+    long long step;
+    double last_ws;
+    int ws_valid, wait_fail;
+};
+
 // Device-resident controller and reduction accumulators of one solve.  The
 // boundary kernel's last block finalises each step here, so a captured CUDA
 // graph can run many steps without the host (dt, t, step, stop flags stay on
@@ -80,6 +89,7 @@ struct DevState {
     unsigned int res_nf, res_arrive;
     long long resid_step;
     unsigned long long t0_ns, done_ns;  // persistent loops: first step taken, run done
+    HostMirror *mirror;                 // mapped host memory, or null
 };
 
 constexpr int kFlagWs = 1;
@@ -312,6 +322,13 @@ __device__ __forceinline__ void step_controller(const Geo &g, DevState *st, long
     }
     st->ws_acc = 0ull;
     st->nf_acc = 0u;
+    if (HostMirror *hm = st->mirror) {
+        if (flags & kFlagWs) hm->last_ws = ws;
+        hm->ws_valid = (flags & kFlagWs) ? 1 : 0;
+        hm->wait_fail = __ldcg(&st->wait_fail);
+        hm->step = nstep;
+        __threadfence_system();
+    }
     __threadfence();
     st->arrive = 0u;
 }

@@ -271,6 +271,10 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
             // a row never arrived: record the failure and stop the run
             atomicExch(&st->wait_fail, 1);
             atomicExch(&st->done, 1);
+            if (st->mirror) {
+                st->mirror->wait_fail = 1;
+                __threadfence_system();
+            }
         }
     }
     if (MPD_PDL_TRIG_INT == 2) pdl_trigger();

@@ -103,6 +103,8 @@ struct mpd_solver {
     unsigned long long *red = nullptr;
     mpd::DevState *st = nullptr;
     mpd::DevState *h_st = nullptr;  // pinned mirror
+    mpd::HostMirror *hm = nullptr;   // mapped pinned: the controller's per-step outputs
+    cudaEvent_t ev_sync = nullptr;   // completion of the enqueued work, for hm
     mpd::SegDesc *d_seg = nullptr;
     int32_t *d_code = nullptr;
     double *d_consts = nullptr;
@@ -125,6 +127,22 @@ int DevAlloc(mpd_solver *s, T **p, size_t count) {
     MPD_CK(cudaMalloc(reinterpret_cast<void **>(p), bytes));
     s->dev_bytes += bytes;
     return MPD_OK;
+}
+
+// Device address of the mapped mirror (null when there is none).
+mpd::HostMirror *DeviceMirror(mpd_solver *s) {
+    void *d = nullptr;
+    if (!s->hm || cudaHostGetDevicePointer(&d, s->hm, 0) != cudaSuccess) return nullptr;
+    return static_cast<mpd::HostMirror *>(d);
+}
+
+// The mirror's fields from the host copy of the state.
+void RefreshMirror(mpd_solver *s) {
+    if (!s->hm) return;
+    s->hm->step = s->h_st->step;
+    s->hm->last_ws = s->h_st->last_ws;
+    s->hm->ws_valid = s->h_st->ws_valid;
+    s->hm->wait_fail = s->h_st->wait_fail;
 }
 
 void FreeAll(mpd_solver *s) {
@@ -150,6 +168,8 @@ void FreeAll(mpd_solver *s) {
     cudaFree(s->d_code);
     cudaFree(s->d_consts);
     if (s->h_st) cudaFreeHost(s->h_st);
+    if (s->hm) cudaFreeHost(s->hm);
+    if (s->ev_sync) cudaEventDestroy(s->ev_sync);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->snap_ev) cudaEventDestroy(s->snap_ev);
@@ -201,6 +221,7 @@ int UploadPhysical(mpd_solver *s, const double *phys10) {
                                    s->ps * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
     }
     mpd::DevState init{};
+    init.mirror = DeviceMirror(s);
     init.T = INFINITY;
     init.max_steps = LLONG_MAX;
     init.want_ws = 1;
@@ -209,6 +230,7 @@ int UploadPhysical(mpd_solver *s, const double *phys10) {
     MPD_CK(cudaMemcpyAsync(s->st, s->h_st, sizeof(mpd::DevState), cudaMemcpyHostToDevice,
                            s->stream));
     MPD_CK(cudaStreamSynchronize(s->stream));
+    RefreshMirror(s);
     s->host_step = 0;
     return MPD_OK;
 }
@@ -271,6 +293,7 @@ int SyncState(mpd_solver *s) {
     MPD_CK(cudaMemcpyAsync(s->h_st, s->st, sizeof(mpd::DevState), cudaMemcpyDeviceToHost,
                            s->stream));
     MPD_CK(cudaStreamSynchronize(s->stream));
+    RefreshMirror(s);
     if (s->h_st->wait_fail)
         return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
     return MPD_OK;
@@ -280,6 +303,7 @@ int PushState(mpd_solver *s) {
     MPD_CK(cudaMemcpyAsync(s->st, s->h_st, sizeof(mpd::DevState), cudaMemcpyHostToDevice,
                            s->stream));
     MPD_CK(cudaStreamSynchronize(s->stream));
+    RefreshMirror(s);
     return MPD_OK;
 }
 
@@ -402,10 +426,14 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     STEP(DevAlloc(s, &s->small, 16));
     STEP(DevAlloc(s, &s->red, 4));
     STEP(DevAlloc(s, &s->st, 1));
-    if (cudaMallocHost(reinterpret_cast<void **>(&s->h_st), sizeof(mpd::DevState)) != cudaSuccess) {
+    if (cudaMallocHost(reinterpret_cast<void **>(&s->h_st), sizeof(mpd::DevState)) != cudaSuccess ||
+        cudaHostAlloc(reinterpret_cast<void **>(&s->hm), sizeof(mpd::HostMirror),
+                      cudaHostAllocMapped) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_sync, cudaEventDisableTiming) != cudaSuccess) {
         FreeAll(s);
         return Fail(MPD_ERR_NOMEM, "pinned allocation failed");
     }
+    std::memset(s->hm, 0, sizeof(mpd::HostMirror));
     // wall profiles + dr (Grid::Build: R = r_outer - r_inner, dr = R / M_max)
     {
         std::vector<double> h(5 * static_cast<size_t>(s->rows));
@@ -691,6 +719,19 @@ int mpd_max_wave_speed(mpd_solver *s, double *out) {
     int rc = CheckHandle(s);
     if (rc != MPD_OK) return rc;
     if (!out) return Fail(MPD_ERR_INVALID, "out is NULL");
+    if (s->hm) {
+        // after a step the controller has left the speed in the mapped
+        // mirror: wait for the enqueued work, no copy of the whole state
+        MPD_CK(cudaEventRecord(s->ev_sync, s->stream));
+        MPD_CK(cudaEventSynchronize(s->ev_sync));
+        const volatile mpd::HostMirror *m = s->hm;
+        if (m->wait_fail)
+            return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
+        if (m->ws_valid && m->step > 0) {
+            *out = m->last_ws;
+            return MPD_OK;
+        }
+    }
     rc = SyncState(s);
     if (rc != MPD_OK) return rc;
     if (s->h_st->ws_valid && s->h_st->step > 0) {
@@ -1114,6 +1155,7 @@ int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *
                                    b->stream));
         MPD_CK(cudaStreamSynchronize(b->stream));
         for (mpd_solver *s : b->solvers) {
+            RefreshMirror(s);
             total += s->h_st->step;
             all_done = all_done && s->h_st->done;
             failed = failed || s->h_st->wait_fail;
