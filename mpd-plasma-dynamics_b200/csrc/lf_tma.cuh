@@ -41,6 +41,12 @@ namespace mpd {
 #ifndef MPD_TMA_MIN_BAND
 #define MPD_TMA_MIN_BAND 1
 #endif
+// L2 eviction priorities on the interior's traffic: the rows a step reads are
+// never read again (the buffer is next overwritten), the cells it writes are
+// the next step's input.
+#ifndef MPD_L2_HINTS
+#define MPD_L2_HINTS 1
+#endif
 
 constexpr int kTmaWarps = MPD_TMA_WARPS;      // warps per block
 constexpr int kTmaStages = MPD_TMA_STAGES;    // rows in flight per warp
@@ -57,6 +63,7 @@ __host__ __device__ inline void tma_band(int L, int nbands, int b, int &l_begin,
 
 struct TmaWarp {
     FastStrip f;
+    uint64_t pol_read, pol_write;  // L2 policies of the loads and stores
     const CUtensorMap *map;
     double *stage;   // kTmaStages rows of [8][32]
     uint32_t bar0;   // shared address of this warp's first barrier
@@ -82,8 +89,13 @@ struct TmaWarp {
         if (lane == 0 && j - jbase < (uint32_t)nrows) {
             const uint32_t s = j % kTmaStages;
             mbar_expect_tx(bar(s), kTmaRowBytes);
+#if MPD_L2_HINTS
+            tma_load_3d_hint(smem_addr(stage + s * kTmaRow), map, bar(s), f.p - lane,
+                             row0 + (int)(j - jbase), 0, pol_read);
+#else
             tma_load_3d(smem_addr(stage + s * kTmaRow), map, bar(s), f.p - lane,
                         row0 + (int)(j - jbase), 0);
+#endif
         }
     }
 
@@ -135,7 +147,13 @@ __device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, uint32_t &j, do
     if (s.out_lane) {
         const size_t i = g.ix(l, s.p);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) s.u[(size_t)k * g.ps + i] = out[k];
+        for (int k = 0; k < 8; ++k) {
+#if MPD_L2_HINTS
+            st_global_hint(s.u + (size_t)k * g.ps + i, out[k], w.pol_write);
+#else
+            s.u[(size_t)k * g.ps + i] = out[k];
+#endif
+        }
         if (wants_central(g.L, g.M, l, s.p)) store_central(s.cphys, s.len, g.L, g.M, l, s.p, out);
     }
     if (WANT_WS) {
@@ -221,6 +239,12 @@ __device__ __forceinline__ void tma_warp_setup(TmaWarp &w, const Geo &g, int str
     s.kz = dt * (0.5 / g.dz);
     w.map = map;
     w.lane = lane;
+#if MPD_L2_HINTS
+    w.pol_read = l2_policy_evict_first();
+    w.pol_write = l2_policy_evict_last();
+#else
+    w.pol_read = w.pol_write = 0;
+#endif
 }
 
 __device__ __forceinline__ unsigned char *tma_smem_base(unsigned char *raw) {

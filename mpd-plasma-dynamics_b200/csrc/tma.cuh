@@ -57,6 +57,25 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
     return true;
 }
 
+// L2 eviction-priority policies (createpolicy): evict_first for data read
+// once, evict_last for data the next kernel reads again.
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// A double store carrying an L2 eviction-priority policy.
+__device__ __forceinline__ void st_global_hint(double *p, double v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol)
+                 : "memory");
+}
+
 __device__ __forceinline__ void tmap_prefetch(const CUtensorMap *map) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
 }
@@ -70,6 +89,16 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
         " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
         "l"(map), "r"(bar), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+// tma_load_3d with an L2 eviction-priority policy.
+__device__ __forceinline__ void tma_load_3d_hint(uint32_t dst, const CUtensorMap *map,
+                                                 uint32_t bar, int x, int y, int z, uint64_t pol) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        ".L2::cache_hint [%0], [%1, {%3, %4, %5}], [%2], %6;" ::"r"(dst),
+        "l"(map), "r"(bar), "r"(x), "r"(y), "r"(z), "l"(pol)
         : "memory");
 }
 
