@@ -234,6 +234,8 @@ def test_bad_config_is_rejected_before_device_work(pkg):
     ("reference_default", cases.reference_default_config(L=80, M=40), 300, 7, 1e300),
     ("edge_segments", cases.edge_config(), 200, 1, 1e300),
     ("t_clamp", cases.channel_config(L=64, M=30, a=0.1), 100000, 10, 0.02),
+    # a square grid with bands of more than ten rows per warp
+    ("square_800x800", cases.channel_config(L=800, M=800, a=0.1), 60, 20, 1e300),
 ])
 def test_persistent_engine_matches_graph_engine(pkg, name, cfg, steps, resid_every, T):
     """One cooperative launch per chunk of steps gives the graph path's bits:
