@@ -230,8 +230,8 @@ MPD_HD void lf_cell_exact(const double U[5][8], const Phys Q[5], const double R[
 // kz = dt / (2 dz), kr = dt / (2 dr_l); Gz / Gr are each equation's z / r
 // flux combination at a point (index 6 of Gz, free because u_7 has no z flux,
 // carries v_z r; index 7 of Gr, free because u_8 has no r flux, carries v_r r;
-// both feed u_5's -p div(r v) source).  Divides become reciprocals computed by
-// Newton iteration from a single-precision seed.
+// both feed u_5's -p div(r v) source).  Divides become reciprocals: the
+// hardware's double-precision seed with one polynomial correction (rcp_nr).
 // ---------------------------------------------------------------------------
 
 // 1/x from a seed y0 = (1 - e) / x: y0 (1 + e + e^2) = (1 - e^3) / x, three
@@ -373,7 +373,7 @@ MPD_HD void fast_finish(const double S[10], const double Un[8], const double Gzn
 }
 
 // Wave speed |v| + c_s + c_a of a new cell state at radius r (ir = 1 / r),
-// with reciprocals and Newton square roots:
+// with reciprocals and seeded square roots (rcp_nr, sqrt_speed):
 //   |v|^2 = (u_2^2 + u_3^2) / u_1^2,  c_s^2 = gamma (gamma - 1) u_5 / u_1,
 //   c_a^2 = (H_z^2 + H_r^2 + H_phi^2) r / u_1   (u_1 = rho r, u_5 = rho e r).
 // The wave speed's square roots, without special cases: the argument is

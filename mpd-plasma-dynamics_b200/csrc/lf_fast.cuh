@@ -12,7 +12,8 @@
 //     cell row, which is added to that row's A at once (S = A + B); a cell row
 //     is closed when the point row after it arrives (fast_finish), so only 19
 //     doubles of state (A of the next row, S of the current one) cross rows;
-//   * divides are Newton reciprocals from the hardware's approximate seed;
+//   * divides are reciprocals from the hardware's approximate seed with one
+//     polynomial correction (rcp_nr);
 //   * a row's geometry (r profiles, dr) is loaded before its conserved values
 //     are waited for, so those loads overlap the wait.
 // The result differs from the exact kernel by rounding only (checked against
