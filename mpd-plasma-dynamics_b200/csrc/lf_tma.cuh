@@ -61,6 +61,42 @@ __host__ __device__ inline void tma_band(int L, int nbands, int b, int &l_begin,
     l_end = 1 + (int)((long long)(b + 1) * L / nbands);
 }
 
+// The first and last strips cost more per row than the others (a per-warp
+// timestamp probe on a B200 at 1600 x 640: 24.1 us per 20-row band against
+// 21.5 us; they store a central column every row).  Their tasks come first,
+// four consecutive bands of one edge strip per block, then the middle
+// strips band by band: that order measured 37.7 us per step against 39.2 us
+// for every strip band by band.  MPD_EDGE_WEIGHT gives the edge strips that
+// percentage of a middle strip's band count; more, shorter edge bands (112,
+// 120) measured no better, so it stays 100.
+#ifndef MPD_EDGE_WEIGHT
+#define MPD_EDGE_WEIGHT 100
+#endif
+
+// Task -> (strip, band, bands of that strip): with three or more strips the
+// first nbands_edge tasks are the first strip's bands, the next nbands_edge
+// the last strip's, the rest the middle strips' (nbands each); otherwise
+// every strip has nbands bands.
+__host__ __device__ inline void tma_task(int task, int nstrips, int nbands, int nbands_edge,
+                                         int &strip, int &band, int &nb) {
+    if (nstrips >= 3) {
+        if (task < 2 * nbands_edge) {
+            strip = task < nbands_edge ? 0 : nstrips - 1;
+            band = task < nbands_edge ? task : task - nbands_edge;
+            nb = nbands_edge;
+            return;
+        }
+        const int u = task - 2 * nbands_edge;
+        strip = 1 + u % (nstrips - 2);
+        band = u / (nstrips - 2);
+        nb = nbands;
+        return;
+    }
+    strip = task % nstrips;
+    band = task / nstrips;
+    nb = nbands;
+}
+
 struct TmaWarp {
     FastStrip f;
     uint64_t pol_read, pol_write;  // L2 policies of the loads and stores
@@ -256,15 +292,15 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
     lf_tma_kernel(Geo g, const __grid_constant__ CUtensorMap map0,
                   const __grid_constant__ CUtensorMap map1, double *buf0, double *buf1,
                   DevState *st, double dt_arg, int use_state_dt, double *cphys, int len,
-                  int nstrips, int nbands) {
+                  int nstrips, int nbands, int nbands_edge) {
     extern __shared__ __align__(128) unsigned char tma_smem_raw[];
     unsigned char *tma_smem = tma_smem_base(tma_smem_raw);
     const int wib = threadIdx.x >> 5;
     const int task = (int)blockIdx.x * kTmaWarps + wib;
-    const int strip = task % nstrips;
-    const int band = task / nstrips;
+    int strip, band, nb;
+    tma_task(task, nstrips, nbands, nbands_edge, strip, band, nb);
     int l_begin = 1, l_end = 1;
-    if (band < nbands) tma_band(g.L, nbands, band, l_begin, l_end);
+    if (band < nb) tma_band(g.L, nb, band, l_begin, l_end);
     const uint32_t bar0 =
         smem_addr(tma_smem + kTmaWarps * kTmaStages * kTmaRowBytes) + 8u * wib * kTmaStages;
     // While the previous kernel of the stream may still run: only this
@@ -311,7 +347,7 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
 
 // Strips and bands for one wave of lf_tma_kernel on this device.
 struct TmaPlan {
-    int nstrips = 0, nbands = 0, blocks = 0;
+    int nstrips = 0, nbands = 0, nbands_edge = 0, blocks = 0;
 };
 
 inline cudaError_t plan_lf_tma(const Geo &g, int device, TmaPlan &plan) {
@@ -329,13 +365,27 @@ inline cudaError_t plan_lf_tma(const Geo &g, int device, TmaPlan &plan) {
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     const int warps = sms * per_sm * kTmaWarps;
-    plan.nstrips = (g.M + kFastCells - 1) / kFastCells;
-    int nb = warps / plan.nstrips;
-    const int min_band = MPD_TMA_MIN_BAND;  // rows; each band re-reads two rows above its first
-    if (nb > g.L / min_band) nb = g.L / min_band;
-    if (nb < 1) nb = 1;
+    const int S = (g.M + kFastCells - 1) / kFastCells;
+    plan.nstrips = S;
+    const int max_nb = g.L / MPD_TMA_MIN_BAND > 1 ? g.L / MPD_TMA_MIN_BAND : 1;
+    int nb, nbe;
+    if (S >= 3) {
+        // (S - 2) nb + 2 nbe <= warps with nbe = nb * weight
+        nb = (int)((long long)warps * 100 / ((long long)(S - 2) * 100 + 2 * MPD_EDGE_WEIGHT));
+        if (nb > max_nb) nb = max_nb;
+        if (nb < 1) nb = 1;
+        nbe = (int)((long long)nb * MPD_EDGE_WEIGHT / 100);
+        if (nbe > max_nb) nbe = max_nb;
+        if (nbe < nb) nbe = nb;
+    } else {
+        nb = warps / S;
+        if (nb > max_nb) nb = max_nb;
+        if (nb < 1) nb = 1;
+        nbe = nb;
+    }
     plan.nbands = nb;
-    const int tasks = plan.nstrips * plan.nbands;
+    plan.nbands_edge = nbe;
+    const int tasks = S >= 3 ? (S - 2) * nb + 2 * nbe : S * nb;
     plan.blocks = (tasks + kTmaWarps - 1) / kTmaWarps;
     return cudaSuccess;
 }
@@ -347,10 +397,10 @@ inline cudaError_t launch_lf_tma(const Geo &g, const TmaPlan &plan, const CUtens
     if (want_ws)
         return launch_pdl(lf_tma_kernel<true>, dim3(plan.blocks), dim3(32 * kTmaWarps), kTmaSmem,
                           stream, g, map0, map1, buf0, buf1, st, dt, use_state_dt, cphys, len,
-                          plan.nstrips, plan.nbands);
+                          plan.nstrips, plan.nbands, plan.nbands_edge);
     return launch_pdl(lf_tma_kernel<false>, dim3(plan.blocks), dim3(32 * kTmaWarps), kTmaSmem,
                       stream, g, map0, map1, buf0, buf1, st, dt, use_state_dt, cphys, len,
-                      plan.nstrips, plan.nbands);
+                      plan.nstrips, plan.nbands, plan.nbands_edge);
 }
 
 }  // namespace mpd
