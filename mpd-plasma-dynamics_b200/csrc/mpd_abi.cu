@@ -41,7 +41,12 @@ int Fail(int code, const std::string &msg) {
     } while (0)
 
 constexpr int kRedBlocks = 592;  // 4 x 148 SMs for the deterministic sums
-constexpr int kBcBlock = 64;     // boundary-ring threads per block
+// Boundary-ring threads per block: measured on a B200, 32 and 128 no better
+// than 64 and 256 2 us a step slower (fewer, fuller SMs lengthen the chains).
+#ifndef MPD_BC_BLOCK
+#define MPD_BC_BLOCK 64
+#endif
+constexpr int kBcBlock = MPD_BC_BLOCK;  // boundary-ring threads per block
 
 // cuTensorMapEncodeTiled, fetched from the driver at run time (no -lcuda).
 using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
