@@ -326,7 +326,8 @@ __device__ __forceinline__ void step_controller(const Geo &g, DevState *st, long
         if (flags & kFlagWs) hm->last_ws = ws;
         hm->ws_valid = (flags & kFlagWs) ? 1 : 0;
         hm->wait_fail = __ldcg(&st->wait_fail);
-        hm->step = nstep;
+        __threadfence_system();  // the fields above before the step number: a
+        hm->step = nstep;        // host that sees the new step sees them too
         __threadfence_system();
     }
     __threadfence();

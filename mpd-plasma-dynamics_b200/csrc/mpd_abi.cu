@@ -2,6 +2,8 @@
 // launch sequence, the graph-resident run loop, diagnostics and transfers.
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -726,10 +728,29 @@ int mpd_max_wave_speed(mpd_solver *s, double *out) {
     if (!out) return Fail(MPD_ERR_INVALID, "out is NULL");
     if (s->hm) {
         // after a step the controller has left the speed in the mapped
-        // mirror: wait for the enqueued work, no copy of the whole state
-        MPD_CK(cudaEventRecord(s->ev_sync, s->stream));
-        MPD_CK(cudaEventSynchronize(s->ev_sync));
+        // mirror, the step number last: watch that word for the step this
+        // handle issued last (its controller's final write), no copy of the
+        // whole state; after 100 ms without it, wait for the stream instead
         const volatile mpd::HostMirror *m = s->hm;
+        const long long want = s->host_step;
+        bool seen = false;
+        if (want > 0) {
+            const auto t0 = std::chrono::steady_clock::now();
+            for (long long spins = 0;; ++spins) {
+                if (m->step >= want || m->wait_fail) {
+                    seen = true;
+                    break;
+                }
+                if ((spins & 1023) == 1023 &&
+                    std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(100))
+                    break;
+            }
+            std::atomic_thread_fence(std::memory_order_acquire);
+        }
+        if (!seen) {
+            MPD_CK(cudaEventRecord(s->ev_sync, s->stream));
+            MPD_CK(cudaEventSynchronize(s->ev_sync));
+        }
         if (m->wait_fail)
             return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
         if (m->ws_valid && m->step > 0) {
