@@ -322,13 +322,17 @@ __device__ __forceinline__ void step_controller(const Geo &g, DevState *st, long
     }
     st->ws_acc = 0ull;
     st->nf_acc = 0u;
-    if (HostMirror *hm = st->mirror) {
+    // per-call mode only: a run's loop is never watched from the host (the
+    // host state, mirror included, is refreshed when the run ends), and a
+    // system-scope fence costs each step ~1.7 us on its critical path
+    // (measured on a B200: a run's step 39.7 -> 36.1 us without the two it had)
+    HostMirror *hm = run_mode ? nullptr : st->mirror;
+    if (hm) {
         if (flags & kFlagWs) hm->last_ws = ws;
         hm->ws_valid = (flags & kFlagWs) ? 1 : 0;
         hm->wait_fail = __ldcg(&st->wait_fail);
         __threadfence_system();  // the fields above before the step number: a
         hm->step = nstep;        // host that sees the new step sees them too
-        __threadfence_system();
     }
     __threadfence();
     st->arrive = 0u;
