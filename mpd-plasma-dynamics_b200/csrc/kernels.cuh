@@ -266,10 +266,29 @@ __device__ __forceinline__ BcView make_bc_view(const Geo &g, const double *u0, d
     return v;
 }
 
+#ifndef MPD_ARRIVE_ACQREL
+#define MPD_ARRIVE_ACQREL 1
+#endif
+
+__device__ __forceinline__ unsigned int atom_add_acq_rel_u32(unsigned int *p, unsigned int v) {
+    unsigned int old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+                 : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // True in thread 0 of the last block of the grid to get here, after every
 // block's writes (state, lines, reduction atomics) are visible to it.  Every
-// thread of every block calls it.
+// thread of every block calls it.  The barrier orders the block's writes
+// before thread 0's release (release is cumulative over what the barrier
+// made visible to it); the arrivals form one read-modify-write chain, so
+// the last one's acquire sees every block's writes.
 __device__ __forceinline__ bool last_block_arrived(DevState *st) {
+#if MPD_ARRIVE_ACQREL
+    __syncthreads();
+    if (threadIdx.x != 0) return false;
+    return atom_add_acq_rel_u32(&st->arrive, 1u) == gridDim.x - 1;
+#else
     __shared__ int is_last;
     __threadfence();
     __syncthreads();
@@ -278,6 +297,7 @@ __device__ __forceinline__ bool last_block_arrived(DevState *st) {
     if (!is_last || threadIdx.x != 0) return false;
     __threadfence();
     return true;
+#endif
 }
 
 // End of step `step` (dt the step used), run by one thread once every cell's
@@ -334,7 +354,11 @@ __device__ __forceinline__ void step_controller(const Geo &g, DevState *st, long
         __threadfence_system();  // the fields above before the step number: a
         hm->step = nstep;        // host that sees the new step sees them too
     }
+    // the next arrivals come from a later launch, which the launch order
+    // places after every store of this one
+#if !MPD_ARRIVE_ACQREL
     __threadfence();
+#endif
     st->arrive = 0u;
 }
 
