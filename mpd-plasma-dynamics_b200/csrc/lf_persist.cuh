@@ -78,20 +78,12 @@ __device__ __forceinline__ bool team_barrier(const TeamCtx &tm) {
         GridSync *gs = tm.gs;
         int ok = 1;
         const unsigned int g0 = ld_acquire_u32(&gs->gen);
-#if MPD_ARRIVE_ACQREL
         // release of the block's writes (cumulative over the barrier above);
         // the last arrival acquires every earlier one through the chain of
         // read-modify-writes, and its release of gen passes them all on
         if (atom_add_acq_rel_u32(&gs->count, 1u) == (unsigned int)tm.size - 1) {
             atomicExch(&gs->count, 0u);
             st_release_u32(&gs->gen, g0 + 1u);
-#else
-        __threadfence();
-        if (atomicAdd(&gs->count, 1u) == (unsigned int)tm.size - 1) {
-            atomicExch(&gs->count, 0u);
-            __threadfence();
-            st_release_u32(&gs->gen, g0 + 1u);
-#endif
         } else if (ld_acquire_u32(&gs->gen) == g0) {
             const unsigned long long t0 = global_ns();
             while (ld_acquire_u32(&gs->gen) == g0) {
