@@ -174,24 +174,25 @@ __device__ __noinline__ void persist_resid_phase(const PersistArgs &a, int par, 
     const Geo &g = a.g;
     const double *un = par ? a.buf0 : a.buf1;  // written by the step that just ended
     const double *uo = par ? a.buf1 : a.buf0;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) key[k] = 0ull;
-    nf = 0u;
+    ResidAcc acc;
+    acc.init();
     const int W = g.M + 1;
     const int total = g.L * W;
     for (int c = rank * (int)blockDim.x + (int)threadIdx.x; c < total;
          c += size * (int)blockDim.x) {
         const size_t i = g.ix(1 + c / W, 1 + c % W);
+        double an[8], ao[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const double an = __ldcg(un + (size_t)k * g.ps + i);
-            const double ao = __ldcg(uo + (size_t)k * g.ps + i);
-            const unsigned long long d = max_key(fabs(an - ao), nf);
-            const unsigned long long o = max_key(fabs(ao), nf);
-            key[k] = d > key[k] ? d : key[k];
-            key[8 + k] = o > key[8 + k] ? o : key[8 + k];
+            an[k] = __ldcg(un + (size_t)k * g.ps + i);
+            ao[k] = __ldcg(uo + (size_t)k * g.ps + i);
         }
+        acc.fold(an, ao);
     }
+    unsigned long long k16[16];
+    acc.keys(k16, nf);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) key[k] = k16[k];
 }
 
 // Per-block working memory of the persistent loops.

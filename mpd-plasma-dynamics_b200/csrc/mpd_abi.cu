@@ -102,6 +102,7 @@ struct mpd_solver {
     double *cphys = nullptr;                 // central lines (boundary inputs)
     double *wall[2] = {nullptr, nullptr};    // wall lines, by step parity
     int len = 0;                             // line length
+    int resid_blocks = 0;                    // residual_kernel: one resident wave
     CUtensorMap tmap[2];                     // conserved planes of buf[0] / buf[1]
     mpd::TmaPlan plan;                       // one-wave strips x bands
     mpd::TmaPlan pplan;                      // persistent launch (cooperative wave)
@@ -290,7 +291,7 @@ int EnqueueStep(mpd_solver *s, bool first, bool use_state_dt, double dt, bool wi
         MPD_CK(cudaGetLastError());
     }
     if (with_residual) {
-        mpd::residual_kernel<<<kRedBlocks, 256, 0, s->stream>>>(g, s->buf[0], s->buf[1], s->st);
+        mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(g, s->buf[0], s->buf[1], s->st);
         MPD_CK(cudaGetLastError());
     }
     return MPD_OK;
@@ -474,6 +475,16 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     g.drin = s->geo + 2 * s->rows;
     g.drout = s->geo + 3 * s->rows;
     g.dr = s->geo + 4 * s->rows;
+    {
+        int sms = 0, per_sm = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mpd::residual_kernel, 256, 0) !=
+                cudaSuccess) {
+            FreeAll(s);
+            return Fail(MPD_ERR_CUDA, "occupancy query for the residual kernel failed");
+        }
+        s->resid_blocks = sms * (per_sm > 0 ? per_sm : 1);
+    }
     if (s->precision == MPD_PRECISION_FAST) {
         for (int b = 0; b < 2; ++b)
             STEP(EncodeStateMap(&s->tmap[b], s->buf[b], s->cols, s->rows, s->pitch, s->ps));
@@ -541,7 +552,7 @@ static int FinishRun(mpd_solver *s, long long step0, mpd_run_stats *stats) {
     MPD_CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     // the residual of the final state, when the loop stopped between checks
     if (!h.resid_valid && h.step > 0) {
-        mpd::residual_kernel<<<kRedBlocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st);
+        mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st);
         MPD_CK(cudaGetLastError());
     }
     rc = SyncState(s);
@@ -851,7 +862,7 @@ int mpd_residual(mpd_solver *s, double *out) {
     int rc = CheckHandle(s);
     if (rc != MPD_OK) return rc;
     if (!out) return Fail(MPD_ERR_INVALID, "out is NULL");
-    mpd::residual_kernel<<<kRedBlocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st);
+    mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st);
     MPD_CK(cudaGetLastError());
     rc = SyncState(s);
     if (rc != MPD_OK) return rc;

@@ -175,6 +175,24 @@ def test_t_clamp_and_residual(pkg):
     solver.close()
 
 
+@pytest.mark.parametrize("L,M", [(200, 80), (40, 63), (33, 95)])
+def test_residual_matches_numpy(pkg, L, M):
+    """The L-inf residual over row x 32-column units: ragged last units
+    (M + 1 = 81, 96) and rows of exactly two units (M + 1 = 64)."""
+    case = cases.channel_case(L=L, M=M)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+    solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=30)
+    before = solver.conserved()
+    solver.Advance(solver.ComputeDt(cfg.dt))
+    after = solver.conserved()
+    inner = (slice(None), slice(1, -1), slice(1, -1))
+    num = np.abs(after[inner] - before[inner]).reshape(8, -1).max(axis=1)
+    den = np.maximum(np.abs(before[inner]).reshape(8, -1).max(axis=1), 1e-300)
+    assert solver.residual() == float((num / den).max())
+    solver.close()
+
+
 def test_restart_set_physical_and_snapshot(pkg):
     case = cases.channel_case(L=24, M=12, a=0.05)
     cfg = case.cfg
