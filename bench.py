@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--cpu-child", type=str, default="", help=argparse.SUPPRESS)
     ap.add_argument("--profile", action="store_true",
                     help="lean run for ncu: warm-up, then --steps eager time steps, no extras")
+    ap.add_argument("--diagnostics", action="store_true",
+                    help="with --profile: then each reduction once (residual, integrals, "
+                         "solution change, outlet, radial symmetry, wave speed)")
     ap.add_argument("--precision", choices=("fast", "exact"), default="fast")
     ap.add_argument("--workload", choices=("plain", "warmstart", "batch", "surrogate", "serve"),
                     default="plain",
@@ -524,7 +527,8 @@ def run_profile(args):
     pkg = __graft_entry__.load_package()
     case = _case()
     cfg = case.cfg
-    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision=args.precision)
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision=args.precision,
+                           with_prev=args.diagnostics)
     # one graph of exactly --warmup steps, so no launch in the profile is an
     # early exit of a graph that ran past the step limit
     w = max(args.warmup, 1)
@@ -533,8 +537,17 @@ def run_profile(args):
     for _ in range(args.steps):
         solver.Advance(dt)
     t, step = solver.time()
+    out = {"profile_steps": args.steps, "step": step, "t": t}
+    if args.diagnostics:
+        out["residual"] = solver.residual()
+        out["integrals"] = [float(x) for x in solver.ComputeIntegrals()]
+        out["change"] = solver.SolutionChange()
+        out["mass_flux"], out["thrust"] = solver.outlet()
+        out["radial"] = solver.CheckRadialSymmetry()
+        solver.set_physical(solver.physical())  # a state with no fused wave speed
+        out["wave_speed"] = solver.MaxWaveSpeed()
     solver.close()
-    print(json.dumps({"profile_steps": args.steps, "step": step, "t": t}))
+    print(json.dumps(out))
 
 
 def run_reference(args, rank, world):

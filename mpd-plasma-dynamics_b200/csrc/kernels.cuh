@@ -675,11 +675,23 @@ __device__ __forceinline__ void block_sum_store(double (&v)[NV], double *partial
     }
 }
 
+// The partials (nblocks x NV) are first copied into shared memory by the
+// whole block (dynamic shared memory of nblocks * NV doubles), then value k
+// is summed by thread k in block order: the same additions as a serial loop
+// over global memory, without a dependent global load per addition.
+__device__ __forceinline__ void stage_partials(const double *partials, int n, double *sh) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sh[i] = partials[i];
+    __syncthreads();
+}
+
 template <int NV>
 __global__ void sum_partials_kernel(const double *partials, int nblocks, double *out) {
+    extern __shared__ double sh_partials[];
+    stage_partials(partials, nblocks * NV, sh_partials);
     if (threadIdx.x >= NV) return;
     double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partials[(size_t)b * NV + threadIdx.x];
+#pragma unroll 8
+    for (int b = 0; b < nblocks; ++b) s += sh_partials[b * NV + threadIdx.x];
     out[threadIdx.x] = s;
 }
 
@@ -741,12 +753,15 @@ __global__ void change_kernel(StateBufs sb, double *prev, double *partials, int 
 // (src/main.cpp:233-247).  Runs as one thread after change_kernel.
 __global__ void change_finish_kernel(const double *partials, int nblocks, DevState *st,
                                      int from_run) {
-    if (threadIdx.x != 0) return;
     if (from_run && !st->check_due) return;
+    extern __shared__ double sh_partials[];
+    stage_partials(partials, 2 * nblocks, sh_partials);
+    if (threadIdx.x != 0) return;
     double sd = 0.0, sc = 0.0;
+#pragma unroll 8
     for (int b = 0; b < nblocks; ++b) {
-        sd += partials[2 * b];
-        sc += partials[2 * b + 1];
+        sd += sh_partials[2 * b];
+        sc += sh_partials[2 * b + 1];
     }
     const double nd = sqrt(sd), nc = sqrt(sc);
     const double change = (nc > 1e-15) ? (nd / nc) : nd;
@@ -761,30 +776,51 @@ __global__ void change_finish_kernel(const double *partials, int nblocks, DevSta
 }
 
 // Diagnostics::GetMassFlux / GetThrust (src/integrals.cpp:45-112): the outlet
-// column is summed serially in m order by one thread, as the reference does.
-__global__ void outlet_kernel(StateBufs sb, double inv_8pi, double *out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// column is summed serially in m order, as the reference does.  The terms of
+// kOutletChunk points are evaluated by the block's threads at once (each
+// with the reference's expression), then thread 0 adds them in m order: the
+// same additions of the same terms as one thread doing everything.
+constexpr int kOutletThreads = 256;
+constexpr int kOutletChunk = 1024;
+__global__ void __launch_bounds__(kOutletThreads) outlet_kernel(StateBufs sb, double inv_8pi,
+                                                                double *out) {
+    __shared__ double tm[kOutletChunk], tt[kOutletChunk];
     const StateView sv = sb.view();
     const Geo &g = sv.g;
     const int l = g.L;
     const double dr_out = g.dr[l];
     double sm = 0.0, sth = 0.0;
-    for (int m_local = 1; m_local <= g.M + 1; ++m_local) {
-        const int m_global = m_local - 1;
-        const double w = (m_global == 0 || m_global == g.M) ? 0.5 : 1.0;
-        const Phys q = sv.phys(l, m_local);
-        const double r = g.r(l, m_local);
-        const double fm = q.rho * q.vz;
-        const double Fm = fm * 2.0 * M_PI * r;
-        sm += w * Fm * dr_out;
-        const double v_z2 = q.vz * q.vz;
-        const double H2 = q.Hz * q.Hz + q.Hr * q.Hr + q.Hphi * q.Hphi;
-        const double ft = q.rho * v_z2 + q.p + H2 * inv_8pi;
-        const double Ft = ft * 2.0 * M_PI * r;
-        sth += w * Ft * dr_out;
+    for (int m0 = 1; m0 <= g.M + 1; m0 += kOutletChunk) {
+        const int n = min(kOutletChunk, g.M + 2 - m0);
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const int m_local = m0 + j;
+            const int m_global = m_local - 1;
+            const double w = (m_global == 0 || m_global == g.M) ? 0.5 : 1.0;
+            const Phys q = sv.phys(l, m_local);
+            const double r = g.r(l, m_local);
+            const double fm = q.rho * q.vz;
+            const double Fm = fm * 2.0 * M_PI * r;
+            tm[j] = w * Fm * dr_out;
+            const double v_z2 = q.vz * q.vz;
+            const double H2 = q.Hz * q.Hz + q.Hr * q.Hr + q.Hphi * q.Hphi;
+            const double ft = q.rho * v_z2 + q.p + H2 * inv_8pi;
+            const double Ft = ft * 2.0 * M_PI * r;
+            tt[j] = w * Ft * dr_out;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+#pragma unroll 8
+            for (int j = 0; j < n; ++j) {
+                sm += tm[j];
+                sth += tt[j];
+            }
+        }
+        __syncthreads();
     }
-    out[0] = sm;
-    out[1] = sth;
+    if (threadIdx.x == 0) {
+        out[0] = sm;
+        out[1] = sth;
+    }
 }
 
 // Materialise the 10 physical planes of the current state (pitched); ghost

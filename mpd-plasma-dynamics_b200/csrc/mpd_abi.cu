@@ -287,7 +287,8 @@ int EnqueueStep(mpd_solver *s, bool first, bool use_state_dt, double dt, bool wi
     if (rc != MPD_OK) return rc;
     if (with_check) {
         mpd::change_kernel<<<kRedBlocks, 256, 0, s->stream>>>(Bufs(s), s->prev, s->partials, 1, 1);
-        mpd::change_finish_kernel<<<1, 32, 0, s->stream>>>(s->partials, kRedBlocks, s->st, 1);
+        mpd::change_finish_kernel<<<1, 256, 2 * kRedBlocks * sizeof(double), s->stream>>>(
+            s->partials, kRedBlocks, s->st, 1);
         MPD_CK(cudaGetLastError());
     }
     if (with_residual) {
@@ -801,7 +802,8 @@ static int ChangeImpl(mpd_solver *s, int save, double *out) {
     if (rc != MPD_OK) return rc;
     if (!s->with_prev) return Fail(MPD_ERR_INVALID, "solver was created without prev planes");
     mpd::change_kernel<<<kRedBlocks, 256, 0, s->stream>>>(Bufs(s), s->prev, s->partials, save, 0);
-    mpd::change_finish_kernel<<<1, 32, 0, s->stream>>>(s->partials, kRedBlocks, s->st, 0);
+    mpd::change_finish_kernel<<<1, 256, 2 * kRedBlocks * sizeof(double), s->stream>>>(
+        s->partials, kRedBlocks, s->st, 0);
     MPD_CK(cudaGetLastError());
     rc = SyncState(s);
     if (rc != MPD_OK) return rc;
@@ -822,7 +824,8 @@ int mpd_integrals(mpd_solver *s, double out7[7]) {
     if (!out7) return Fail(MPD_ERR_INVALID, "out is NULL");
     const int nb = s->L < kRedBlocks ? s->L : kRedBlocks;
     mpd::integrals_kernel<<<nb, 256, 0, s->stream>>>(Bufs(s), s->partials);
-    mpd::sum_partials_kernel<7><<<1, 32, 0, s->stream>>>(s->partials, nb, s->small);
+    mpd::sum_partials_kernel<7><<<1, 256, 7 * nb * sizeof(double), s->stream>>>(s->partials, nb,
+                                                                               s->small);
     MPD_CK(cudaGetLastError());
     MPD_CK(cudaMemcpyAsync(out7, s->small, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     MPD_CK(cudaStreamSynchronize(s->stream));
@@ -834,7 +837,7 @@ int mpd_outlet(mpd_solver *s, double *mass_flux, double *thrust) {
     if (rc != MPD_OK) return rc;
     if (!mass_flux || !thrust) return Fail(MPD_ERR_INVALID, "out is NULL");
     const double inv_8pi = 1.0 / (8.0 * M_PI);
-    mpd::outlet_kernel<<<1, 32, 0, s->stream>>>(Bufs(s), inv_8pi, s->small);
+    mpd::outlet_kernel<<<1, mpd::kOutletThreads, 0, s->stream>>>(Bufs(s), inv_8pi, s->small);
     MPD_CK(cudaGetLastError());
     double h[2];
     MPD_CK(cudaMemcpyAsync(h, s->small, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
