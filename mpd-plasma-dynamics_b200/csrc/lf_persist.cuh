@@ -128,6 +128,14 @@ struct PersistRun {
     int adaptive, resid_every;
 };
 
+// Resident blocks per SM the persistent kernels' register budget is cut for.
+// Two (255 registers, the ring code nearly spill-free) shortens a team's step
+// by a quarter (B200: 100 x 40 on one block 85 -> 66 us, 400 x 160 on four
+// 239 -> 178 us) but a wave then holds 296 blocks instead of 444, and the
+// batched sweep measured 7.47 against 8.09 solves/s; three stays.
+#ifndef MPD_PERSIST_MINB
+#define MPD_PERSIST_MINB MPD_TMA_MINB
+#endif
 constexpr int kPersistThreads = 32 * kTmaWarps;
 constexpr int kPersistSmem = kTmaSmem + kMaxSegments * (int)sizeof(SegDesc);
 
@@ -390,7 +398,7 @@ __device__ __forceinline__ void persist_warp_init(TmaWarp &w, const PersistBlock
 }
 
 // One solve, the whole grid as one team.
-__global__ void __launch_bounds__(kPersistThreads, MPD_TMA_MINB)
+__global__ void __launch_bounds__(kPersistThreads, MPD_PERSIST_MINB)
     lf_persist_kernel(const __grid_constant__ CUtensorMap map0,
                       const __grid_constant__ CUtensorMap map1,
                       const __grid_constant__ PersistArgs a, GridSync *gs) {
@@ -419,7 +427,7 @@ struct BatchArgs {
     int nteams;
 };
 
-__global__ void __launch_bounds__(kPersistThreads, MPD_TMA_MINB)
+__global__ void __launch_bounds__(kPersistThreads, MPD_PERSIST_MINB)
     lf_batch_kernel(const __grid_constant__ BatchArgs b) {
     extern __shared__ __align__(128) unsigned char persist_smem[];
     __shared__ PersistRun run;
