@@ -71,7 +71,7 @@ def parse():
 
 
 def workload_config():
-    return {"workload": "plain FP64 LF time step, coaxial channel 1600x640 (config 2 grid)",
+    return {"workload": "plain FP64 LF time step, straight coaxial channel 1600x640",
             "L_max": L_MAX, "M_max": M_MAX, "cells_per_step": CELLS, "cfl": 0.4,
             "adaptive_dt": True, "precision": "fast", "geometry": "r1=0.2, r2=0.8",
             "l2": "per-step working set 138 MB (8 planes read + 8 written) > 126 MB L2, no flush",
@@ -378,7 +378,7 @@ def run_warmstart(args):
 
 
 def run_serve(args):
-    """Config 5 of the north star, bounded: a large converging-diverging
+    """The serving mix, bounded: a large converging-diverging
     channel warm-started from the surrogate (coarse prediction remapped on
     the device) in one persistent launch beside small sweep solves admitted by
     a device-memory budget; the same mix cold for comparison."""

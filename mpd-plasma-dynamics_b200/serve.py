@@ -1,4 +1,4 @@
-"""Large grid plus a serving mix (config 5 of the north star): one large solve
+"""Large grid plus a serving mix: one large solve
 warm-started from the surrogate's coarse prediction, remapped onto its grid
 by the device bilinear remap, running in the same persistent cooperative
 launch as a batch of small uneven solves admitted by a device-memory budget.

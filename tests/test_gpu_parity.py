@@ -219,8 +219,8 @@ def test_restart_set_physical_and_snapshot(pkg):
     other.close()
 
 
-def test_config2_size_fast_vs_oracle(pkg):
-    """Full config-2 grid (1600 x 640): fast path vs the oracle over 30 steps."""
+def test_full_size_channel_fast_vs_oracle(pkg):
+    """The 1600 x 640 channel: fast path vs the oracle over 30 steps."""
     case = cases.channel_case(L=1600, M=640)
     cfg = case.cfg
     solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
