@@ -193,6 +193,28 @@ def test_residual_matches_numpy(pkg, L, M):
     solver.close()
 
 
+def test_residual_leaves_nan_out_and_flags_it(pkg):
+    """A NaN in the state: the residual's maxima skip it (NaN-ignoring
+    maxima, as numpy's nanmax) and the state is flagged non-finite."""
+    case = cases.channel_case(L=40, M=20)
+    cfg = case.cfg
+    phys = np.array(case.phys, copy=True)
+    phys[0, 20, 10] = np.nan
+    solver = pkg.GpuSolver(cfg, case.grid, phys, precision="fast")
+    before = solver.conserved()
+    solver.Advance(cfg.dt)
+    after = solver.conserved()
+    inner = (slice(None), slice(1, -1), slice(1, -1))
+    assert np.isnan(after[inner]).any() and np.isfinite(after[inner]).any()
+    with np.errstate(invalid="ignore"):
+        num = np.nanmax(np.abs(after[inner] - before[inner]).reshape(8, -1), axis=1)
+        den = np.maximum(np.nanmax(np.abs(before[inner]).reshape(8, -1), axis=1), 1e-300)
+    assert solver.residual() == float(np.nanmax(num / den))
+    res = solver.run(T=1e300, dt=cfg.dt, adaptive=False, max_steps=1)
+    assert res.status == pkg._native.MPD_ERR_NONFINITE
+    solver.close()
+
+
 def test_restart_set_physical_and_snapshot(pkg):
     case = cases.channel_case(L=24, M=12, a=0.05)
     cfg = case.cfg
