@@ -37,6 +37,7 @@ extern "C" {
 #define MPD_ERR_NONFINITE 6      /* NaN or Inf seen in the state                */
 #define MPD_ERR_TIMEOUT 7        /* a bounded device wait gave up               */
 #define MPD_ERR_NO_DEVICE 8      /* no CUDA device / extension unusable         */
+#define MPD_ERR_UNSUPPORTED_IC 9 /* initial condition the device can't evaluate */
 
 /* ---- enumerations (values equal the reference's enums) ----------------- */
 /* FaceBC::Face, include/face_bc.hpp:52 */
@@ -98,7 +99,9 @@ typedef struct mpd_solver mpd_solver;
  * Grid::Build and the Solver ctor (src/solver.cpp:9-16: FaceBC::FromConfig,
  * PerFieldBC validation and expression compile).  phys10 is the initial
  * physical state written by IInitialCondition::Apply: 10 dense host planes in
- * MPD_RHO..MPD_H_PHI order (ghost entries are ignored and treated as 0). */
+ * MPD_RHO..MPD_H_PHI order (ghost entries are ignored and treated as 0);
+ * NULL starts from all-zero planes, for a state set next by
+ * mpd_set_expression_ic or mpd_set_physical. */
 int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *phys10,
                mpd_solver **out);
 void mpd_destroy(mpd_solver *s);
@@ -192,6 +195,15 @@ int mpd_snapshot_wait(mpd_solver *s);
 /* Replace the state by new physical planes (restart; IInitialCondition::Apply
  * + Fields::InitConservative).  Resets step and time to 0. */
 int mpd_set_physical(mpd_solver *s, const double *phys10);
+/* ExpressionIC::Apply (src/ics/expression_ic.cpp:286-324) evaluated on the
+ * device, one thread per cell, with the expressions and user constants of
+ * mpd_expression_ic, then Fields::InitConservative; resets step and time to
+ * 0.  The planes equal mpd_expression_ic's bit for bit (CUDA's math library
+ * stands in for glibc in transcendental functions).  An expression that
+ * reads a field evaluated after it (in the reference's sequential sweep, the
+ * previous cell's value) is refused with MPD_ERR_UNSUPPORTED_IC. */
+int mpd_set_expression_ic(mpd_solver *s, const char *const exprs[8], int n_vars,
+                          const char *const *var_names, const double *var_values);
 
 /* The handle's CUDA stream (a cudaStream_t), for callers that time or order
  * work around the solver. */

@@ -22,11 +22,12 @@ MPD_ERR_EXPR = 5
 MPD_ERR_NONFINITE = 6
 MPD_ERR_TIMEOUT = 7
 MPD_ERR_NO_DEVICE = 8
+MPD_ERR_UNSUPPORTED_IC = 9
 
 STATUS_NAMES = {
     0: "MPD_OK", 1: "MPD_ERR_INVALID", 2: "MPD_ERR_CUDA", 3: "MPD_ERR_NOMEM",
     4: "MPD_ERR_UNSUPPORTED_BC", 5: "MPD_ERR_EXPR", 6: "MPD_ERR_NONFINITE",
-    7: "MPD_ERR_TIMEOUT", 8: "MPD_ERR_NO_DEVICE",
+    7: "MPD_ERR_TIMEOUT", 8: "MPD_ERR_NO_DEVICE", 9: "MPD_ERR_UNSUPPORTED_IC",
 }
 
 FACE_L_LO, FACE_L_HI, FACE_M_LO, FACE_M_HI = 0, 1, 2, 3
@@ -121,6 +122,8 @@ SIGNATURES = [
     ("mpd_snapshot_async", C.c_int, [_VP, DP]),
     ("mpd_snapshot_wait", C.c_int, [_VP]),
     ("mpd_set_physical", C.c_int, [_VP, DP]),
+    ("mpd_set_expression_ic", C.c_int, [_VP, C.POINTER(C.c_char_p), C.c_int,
+                                        C.POINTER(C.c_char_p), DP]),
     ("mpd_get_stream", C.c_int, [_VP, C.POINTER(_VP)]),
     ("mpd_device_bytes", C.c_int, [_VP, C.POINTER(C.c_size_t)]),
     ("mpd_profile_kernels", C.c_int, [_VP, C.c_int, C.c_double, DP]),

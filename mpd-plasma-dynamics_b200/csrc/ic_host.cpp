@@ -13,9 +13,63 @@
 
 namespace mpd {
 void SetLastError(const std::string &msg);
+static const char *kIcNames[8] = {"rho", "v_z", "v_r", "v_phi", "H_z", "H_r", "H_phi", "e"};
 }
 
 using mpd::SetLastError;
+
+namespace mpd {
+
+int CompileIc(const char *const exprs[8], int n_vars, const char *const *var_names,
+              const double *var_values, ExprCode code[8], std::string &err) {
+    // ExpressionIC::Impl symbol table (src/ics/expression_ic.cpp:84-126)
+    static const char *kReserved[] = {"gamma", "beta", "H_z0", "r_0", "z", "r", "r_z", "pi",
+                                      "rho", "v_z", "v_r", "v_phi", "H_z", "H_r", "H_phi", "e"};
+    const std::vector<std::string> syms = {"gamma", "beta", "H_z0", "r_0", "z", "r", "r_z",
+                                           "rho", "v_z", "v_r", "v_phi", "H_z", "H_r", "H_phi", "e"};
+    std::map<std::string, double> consts = {{"pi", M_PI}};
+    for (int i = 0; i < n_vars; ++i) {
+        const std::string name = var_names[i];
+        for (const char *res : kReserved) {
+            if (name == res) {
+                err = "ExpressionIC: user variable '" + name + "' shadows the built-in symbol '" +
+                      res + "'. Choose a different name.";
+                return MPD_ERR_INVALID;
+            }
+        }
+        if (consts.count(name)) {
+            err = "ExpressionIC: failed to register user variable '" + name +
+                  "' (name may already be taken by exprtk).";
+            return MPD_ERR_INVALID;
+        }
+        consts[name] = var_values[i];
+    }
+    // defaults of src/ics/expression_ic.cpp:263-270, evaluation order
+    static const char *kDefaults[8] = {"1.0", "0.0", "0.0", "0.0", "H_z0", "H_z * r_z",
+                                       "(1 - 0.9 * z) * r_0 / r", "beta / (2 * (gamma - 1))"};
+    for (int j = 0; j < 8; ++j) {
+        const std::string src = (exprs && exprs[j]) ? exprs[j] : kDefaults[j];
+        std::string perr;
+        if (!CompileExpr(src, syms, consts, code[j], perr)) {
+            err = std::string("ExpressionIC: failed to compile expression for '") + kIcNames[j] +
+                  "':\n  expression : " + src + "\n  errors     :\n    [1] " + perr;
+            return MPD_ERR_EXPR;
+        }
+    }
+    return MPD_OK;
+}
+
+int IcForwardReference(const ExprCode code[8], int &read_field) {
+    for (int j = 0; j < 8; ++j)
+        for (int v : code[j].vars_used)
+            if (v >= IC_F0 + j && v < IC_COUNT) {
+                read_field = v - IC_F0;
+                return j;
+            }
+    return -1;
+}
+
+}  // namespace mpd
 
 extern "C" int mpd_expression_ic(const mpd_config *cfg, const mpd_geometry *geom,
                                  const char *const exprs[8], int n_vars,
@@ -31,45 +85,15 @@ extern "C" int mpd_expression_ic(const mpd_config *cfg, const mpd_geometry *geom
         SetLastError(err);
         return rc;
     }
-    // ExpressionIC::Impl symbol table (src/ics/expression_ic.cpp:84-126)
-    static const char *kReserved[] = {"gamma", "beta", "H_z0", "r_0", "z", "r", "r_z", "pi",
-                                      "rho", "v_z", "v_r", "v_phi", "H_z", "H_r", "H_phi", "e"};
-    const std::vector<std::string> syms = {"gamma", "beta", "H_z0", "r_0", "z", "r", "r_z",
-                                           "rho", "v_z", "v_r", "v_phi", "H_z", "H_r", "H_phi", "e"};
-    enum { S_GAMMA, S_BETA, S_HZ0, S_R0, S_Z, S_R, S_RZ, S_F0 };
-    std::map<std::string, double> consts = {{"pi", M_PI}};
-    for (int i = 0; i < n_vars; ++i) {
-        const std::string name = var_names[i];
-        for (const char *res : kReserved) {
-            if (name == res) {
-                SetLastError("ExpressionIC: user variable '" + name +
-                             "' shadows the built-in symbol '" + res +
-                             "'. Choose a different name.");
-                return MPD_ERR_INVALID;
-            }
-        }
-        if (consts.count(name)) {
-            SetLastError("ExpressionIC: failed to register user variable '" + name +
-                         "' (name may already be taken by exprtk).");
-            return MPD_ERR_INVALID;
-        }
-        consts[name] = var_values[i];
-    }
-    // defaults of src/ics/expression_ic.cpp:263-270, evaluation order
-    static const char *kDefaults[8] = {"1.0", "0.0", "0.0", "0.0", "H_z0", "H_z * r_z",
-                                       "(1 - 0.9 * z) * r_0 / r", "beta / (2 * (gamma - 1))"};
-    static const char *kNames[8] = {"rho", "v_z", "v_r", "v_phi", "H_z", "H_r", "H_phi", "e"};
     mpd::ExprCode code[8];
-    for (int j = 0; j < 8; ++j) {
-        const std::string src = (exprs && exprs[j]) ? exprs[j] : kDefaults[j];
-        std::string perr;
-        if (!mpd::CompileExpr(src, syms, consts, code[j], perr)) {
-            SetLastError(std::string("ExpressionIC: failed to compile expression for '") +
-                         kNames[j] + "':\n  expression : " + src + "\n  errors     :\n    [1] " +
-                         perr);
-            return MPD_ERR_EXPR;
-        }
+    rc = mpd::CompileIc(exprs, n_vars, var_names, var_values, code, err);
+    if (rc != MPD_OK) {
+        SetLastError(err);
+        return rc;
     }
+    enum { S_GAMMA = mpd::IC_GAMMA, S_BETA = mpd::IC_BETA, S_HZ0 = mpd::IC_HZ0,
+           S_R0 = mpd::IC_R0, S_Z = mpd::IC_Z, S_R = mpd::IC_R, S_RZ = mpd::IC_RZ,
+           S_F0 = mpd::IC_F0 };
     const int L = cfg->L_max, M = cfg->M_max, rows = L + 2, cols = M + 3;
     const size_t n = static_cast<size_t>(rows) * cols;
     std::memset(phys10_out, 0, 10 * n * sizeof(double));

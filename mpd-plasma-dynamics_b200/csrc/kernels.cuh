@@ -849,6 +849,48 @@ __global__ void phys_planes_kernel(StateBufs sb, double *out) {
 }
 
 // Wall lines of step 0: the initial condition on columns 1 and M+1.
+// ExpressionIC::Apply (src/ics/expression_ic.cpp:286-324) on the device:
+// one thread per cell, the compiled programs of the 8 fields in evaluation
+// order, then p and P, into the 10 pitched physical planes (ghost cells
+// stay as they are).  The same arithmetic as the host sweep (mpd_expression_ic)
+// for every program that reads only earlier fields of its cell; the caller
+// refuses the others.
+struct IcPrograms {
+    const int32_t *code;
+    const double *consts;
+    int code_off[8], const_off[8];
+};
+
+__global__ void expression_ic_kernel(Geo g, double *ic, IcPrograms pr) {
+    const int W = g.M + 1;
+    const long long total = (long long)g.L * W;
+    const int plane_of[8] = {P_RHO, P_VZ, P_VR, P_VPHI, P_HZ, P_HR, P_HPHI, P_E};
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int l = 1 + (int)(c / W), m = 1 + (int)(c % W);
+        const int l_global = l - 1, m_global = m - 1;
+        double sym[IC_COUNT];
+        sym[IC_GAMMA] = g.gamma;
+        sym[IC_BETA] = g.beta;
+        sym[IC_HZ0] = g.H_z0;
+        sym[IC_R0] = g.r_0;
+        const double frac = m_global * g.dy;
+        sym[IC_Z] = l_global * g.dz;
+        sym[IC_R] = (1.0 - frac) * g.rin[l] + frac * g.rout[l];
+        sym[IC_RZ] = (1.0 - frac) * g.drin[l] + frac * g.drout[l];
+        for (int j = 0; j < 8; ++j) sym[IC_F0 + j] = 0.0;
+        for (int j = 0; j < 8; ++j)
+            sym[IC_F0 + j] = eval_code(pr.code + pr.code_off[j], pr.consts + pr.const_off[j], sym);
+        const size_t i = g.ix(l, m);
+        for (int j = 0; j < 8; ++j) ic[(size_t)plane_of[j] * g.ps + i] = sym[IC_F0 + j];
+        const double rho = sym[IC_F0 + 0], e = sym[IC_F0 + 7];
+        const double Hz = sym[IC_F0 + 4], Hr = sym[IC_F0 + 5], Hphi = sym[IC_F0 + 6];
+        const double p = (g.gamma - 1.0) * rho * e;
+        ic[(size_t)P_PG * g.ps + i] = p;
+        ic[(size_t)P_PT * g.ps + i] = p + 0.5 * (Hz * Hz + Hr * Hr + Hphi * Hphi);
+    }
+}
+
 __global__ void init_wall_kernel(Geo g, const double *ic, double *wall0, int len) {
     for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < g.L + 2; l += gridDim.x * blockDim.x) {
         const bool in = l >= 1 && l <= g.L;

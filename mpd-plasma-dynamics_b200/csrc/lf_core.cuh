@@ -49,6 +49,10 @@ enum BcSym {
     BS_COUNT = BS_CUR0 + 8
 };
 
+// Expression initial-condition symbols (ExpressionIC::Impl,
+// src/ics/expression_ic.cpp:84-126): the fields in evaluation order.
+enum IcSym { IC_GAMMA = 0, IC_BETA, IC_HZ0, IC_R0, IC_Z, IC_R, IC_RZ, IC_F0, IC_COUNT = IC_F0 + 8 };
+
 struct Phys {
     double rho, vz, vr, vphi, e, p, P, Hz, Hr, Hphi;
 };

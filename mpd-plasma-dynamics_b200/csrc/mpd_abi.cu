@@ -199,16 +199,25 @@ mpd::StateBufs Bufs(const mpd_solver *s) {
 
 // Upload dense host planes (interior only) into pitched device planes and
 // rebuild the conserved state (Fields::InitConservative).
+int InitFromIc(mpd_solver *s);
+
+// The initial physical planes from the host (NULL: all zero), then InitFromIc.
 int UploadPhysical(mpd_solver *s, const double *phys10) {
     const size_t n = static_cast<size_t>(s->rows) * s->cols;
     MPD_CK(cudaMemsetAsync(s->ic, 0, 10 * s->ps * sizeof(double), s->stream));
-    for (int k = 0; k < 10; ++k) {
+    for (int k = 0; phys10 && k < 10; ++k) {
         const double *src = phys10 + k * n + s->cols + 1;  // (l=1, m=1)
         double *dst = s->ic + k * s->ps + s->pitch + 1;
         MPD_CK(cudaMemcpy2DAsync(dst, s->pitch * sizeof(double), src, s->cols * sizeof(double),
                                  (s->M + 1) * sizeof(double), s->L, cudaMemcpyHostToDevice,
                                  s->stream));
     }
+    return InitFromIc(s);
+}
+
+// Fields::InitConservative, the boundary lines, SavePrev and a fresh
+// controller from the initial physical planes in s->ic.
+int InitFromIc(mpd_solver *s) {
     MPD_CK(cudaMemsetAsync(s->buf[0], 0, 8 * s->ps * sizeof(double), s->stream));
     MPD_CK(cudaMemsetAsync(s->buf[1], 0, 8 * s->ps * sizeof(double), s->stream));
     mpd::init_conservative_kernel<<<4 * 148, 256, 0, s->stream>>>(s->g, s->ic, s->buf[0]);
@@ -385,7 +394,7 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     *out = nullptr;
     int rc = mpd::ValidateConfig(cfg, geom, err);
     if (rc != MPD_OK) return Fail(rc, err);
-    if (!geom || !phys10) return Fail(MPD_ERR_INVALID, "geometry and initial planes are required");
+    if (!geom) return Fail(MPD_ERR_INVALID, "geometry is required");
     mpd::CompiledBc cbc;
     rc = mpd::CompileBc(*cfg, cbc, err);
     if (rc != MPD_OK) return Fail(rc, err);
@@ -976,6 +985,66 @@ int mpd_set_physical(mpd_solver *s, const double *phys10) {
     if (s->snap_pending) MPD_CK(cudaEventSynchronize(s->snap_ev));
     s->snap_pending = false;
     return UploadPhysical(s, phys10);
+}
+
+int mpd_set_expression_ic(mpd_solver *s, const char *const exprs[8], int n_vars,
+                          const char *const *var_names, const double *var_values) {
+    int rc = CheckHandle(s);
+    if (rc != MPD_OK) return rc;
+    if (n_vars < 0 || (n_vars > 0 && (!var_names || !var_values)))
+        return Fail(MPD_ERR_INVALID, "mpd_set_expression_ic: bad user variables");
+    std::string err;
+    mpd::ExprCode code[8];
+    rc = mpd::CompileIc(exprs, n_vars, var_names, var_values, code, err);
+    if (rc != MPD_OK) return Fail(rc, err);
+    int read = -1;
+    const int fwd = mpd::IcForwardReference(code, read);
+    if (fwd >= 0) {
+        static const char *names[8] = {"rho", "v_z", "v_r", "v_phi", "H_z", "H_r", "H_phi", "e"};
+        return Fail(MPD_ERR_UNSUPPORTED_IC,
+                    std::string("ExpressionIC on the device: the expression for '") + names[fwd] +
+                        "' reads '" + names[read] +
+                        "', which is evaluated after it; in the reference's sequential sweep "
+                        "that reads the previous cell's value (mpd_expression_ic reproduces it)");
+    }
+    mpd::IcPrograms pr{};
+    std::vector<int32_t> all_code;
+    std::vector<double> all_consts;
+    for (int j = 0; j < 8; ++j) {
+        pr.code_off[j] = static_cast<int>(all_code.size());
+        pr.const_off[j] = static_cast<int>(all_consts.size());
+        all_code.insert(all_code.end(), code[j].code.begin(), code[j].code.end());
+        all_consts.insert(all_consts.end(), code[j].consts.begin(), code[j].consts.end());
+    }
+    if (all_consts.empty()) all_consts.push_back(0.0);
+    MPD_CK(cudaStreamSynchronize(s->stream));
+    if (s->snap_pending) MPD_CK(cudaEventSynchronize(s->snap_ev));
+    s->snap_pending = false;
+    int32_t *d_code = nullptr;
+    double *d_consts = nullptr;
+    if (cudaMalloc(&d_code, all_code.size() * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&d_consts, all_consts.size() * sizeof(double)) != cudaSuccess) {
+        cudaFree(d_code);
+        cudaGetLastError();
+        return Fail(MPD_ERR_NOMEM, "mpd_set_expression_ic: device allocation failed");
+    }
+    cudaError_t e = cudaMemcpyAsync(d_code, all_code.data(), all_code.size() * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_consts, all_consts.data(), all_consts.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->ic, 0, 10 * s->ps * sizeof(double), s->stream);
+    if (e == cudaSuccess) {
+        pr.code = d_code;
+        pr.consts = d_consts;
+        mpd::expression_ic_kernel<<<4 * 148, 256, 0, s->stream>>>(s->g, s->ic, pr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(d_code);
+    cudaFree(d_consts);
+    if (e != cudaSuccess) return Fail(MPD_ERR_CUDA, cudaGetErrorString(e));
+    return InitFromIc(s);
 }
 
 int mpd_get_stream(mpd_solver *s, void **stream) {

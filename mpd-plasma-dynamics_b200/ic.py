@@ -32,7 +32,10 @@ class ExpressionIC(IInitialCondition):
     ``params`` is the ``initial_conditions`` YAML map: one scalar expression
     (or number) per field, optional ``vars`` of user constants.  Missing
     fields take the reference's defaults.  Evaluated on the host by the
-    library's expression compiler, one sequential sweep as in the reference.
+    library's expression compiler: on the device, one thread per cell, when
+    ``GpuSolver`` is given the IC itself (the same bits), or as one
+    sequential host sweep (``Apply``), which also reproduces expressions that
+    read a field evaluated after them.
     """
 
     def __init__(self, params: dict | None = None):
@@ -58,20 +61,32 @@ class ExpressionIC(IInitialCondition):
                     raise ConfigError(f"ExpressionIC: value for var '{k}' must be a scalar number.")
                 self.vars[str(k)] = float(v)
 
-    def Apply(self, grid, cfg: SimConfig) -> np.ndarray:
-        lib = N.load()
-        cc = CConfig(cfg, grid.r_0, N.PRECISION_EXACT, False)
-        keep = [np.ascontiguousarray(a) for a in grid.profiles()]
-        geo = N.Geometry(*(a.ctypes.data_as(N.DP) for a in keep))
+    def _c_args(self):
         exprs = (C.c_char_p * 8)(*[self.exprs[n].encode() if n in self.exprs else None
                                    for n in IC_FIELDS])
         names = (C.c_char_p * max(len(self.vars), 1))(*[k.encode() for k in self.vars])
         vals = np.array(list(self.vars.values()) or [0.0], dtype=np.float64)
+        return exprs, len(self.vars), names, vals
+
+    def Apply(self, grid, cfg: SimConfig) -> np.ndarray:
+        """The 10 physical planes on the host (one sequential sweep)."""
+        lib = N.load()
+        cc = CConfig(cfg, grid.r_0, N.PRECISION_EXACT, False)
+        keep = [np.ascontiguousarray(a) for a in grid.profiles()]
+        geo = N.Geometry(*(a.ctypes.data_as(N.DP) for a in keep))
+        exprs, n_vars, names, vals = self._c_args()
         out = np.zeros((10, cfg.L_max + 2, cfg.M_max + 3))
-        rc = lib.mpd_expression_ic(cc.ptr, C.byref(geo), exprs, len(self.vars), names,
+        rc = lib.mpd_expression_ic(cc.ptr, C.byref(geo), exprs, n_vars, names,
                                    vals.ctypes.data_as(N.DP), out.ctypes.data_as(N.DP))
         N.check(rc, lib)
         return out
+
+    def ApplyDevice(self, lib, handle) -> int:
+        """Evaluate into a solver's device state (mpd_set_expression_ic); the
+        status, MPD_ERR_UNSUPPORTED_IC for expressions that read a field
+        evaluated after them."""
+        exprs, n_vars, names, vals = self._c_args()
+        return lib.mpd_set_expression_ic(handle, exprs, n_vars, names, vals.ctypes.data_as(N.DP))
 
     def Name(self):
         return "expression"

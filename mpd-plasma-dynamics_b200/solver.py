@@ -54,7 +54,12 @@ class GpuSolver:
         self.lib = N.load()
         self.cfg = cfg
         self.grid = grid
-        phys = ArrayIC(ic).Apply(grid, cfg) if isinstance(ic, np.ndarray) else ic.Apply(grid, cfg)
+        # an expression IC is evaluated on the device after creation
+        on_device = isinstance(ic, ExpressionIC)
+        if isinstance(ic, np.ndarray):
+            phys = ArrayIC(ic).Apply(grid, cfg)
+        else:
+            phys = None if on_device else ic.Apply(grid, cfg)
         self.shape = (cfg.L_max + 2, cfg.M_max + 3)
         if with_prev is None:
             with_prev = cfg.convergence_threshold > 0.0
@@ -62,11 +67,21 @@ class GpuSolver:
         self._cc = CConfig(cfg, grid.r_0, PRECISIONS[precision], with_prev)
         self._prof = [np.ascontiguousarray(a, dtype=np.float64) for a in grid.profiles()]
         geo = N.Geometry(*(_dp(a) for a in self._prof))
-        phys = np.ascontiguousarray(phys, dtype=np.float64)
+        if phys is not None:
+            phys = np.ascontiguousarray(phys, dtype=np.float64)
         h = C.c_void_p()
-        N.check(self.lib.mpd_create(self._cc.ptr, C.byref(geo), _dp(phys), C.byref(h)), self.lib)
+        N.check(self.lib.mpd_create(self._cc.ptr, C.byref(geo),
+                                    _dp(phys) if phys is not None else None, C.byref(h)), self.lib)
         self.h = h
         self.precision = precision
+        if on_device:
+            rc = ic.ApplyDevice(self.lib, self.h)
+            if rc == N.MPD_ERR_UNSUPPORTED_IC:
+                # order-dependent expressions: the reference's sequential sweep
+                self.set_physical(ic.Apply(grid, cfg))
+            elif rc != N.MPD_OK:
+                self.close()
+                N.check(rc, self.lib)
 
     # -- lifetime -------------------------------------------------------------
     def close(self):
