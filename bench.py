@@ -49,13 +49,15 @@ def parse():
                     help="with --profile: then each reduction once (residual, integrals, "
                          "solution change, outlet, radial symmetry, wave speed)")
     ap.add_argument("--precision", choices=("fast", "exact"), default="fast")
-    ap.add_argument("--workload", choices=("plain", "warmstart", "batch", "surrogate", "serve"),
+    ap.add_argument("--workload", choices=("plain", "warmstart", "batch", "surrogate", "serve",
+                                           "converge"),
                     default="plain",
                     help="plain: the 1600x640 time step (default); warmstart: surrogate-warm-"
                          "started batched steady solves vs the plain time march; batch: the "
                          "batched sweep of uneven grids; surrogate: training iterations of "
                          "the warm-start network; serve: a large warm-started grid beside a "
-                         "memory-budgeted batch of small solves")
+                         "memory-budgeted batch of small solves; converge: the 1600x640 "
+                         "channel time-marched to an L-inf residual of 1e-8 (--max-steps)")
     ap.add_argument("--n-train", type=int, default=2000)
     ap.add_argument("--n-eval", type=int, default=256)
     ap.add_argument("--epochs", type=int, default=60)
@@ -377,6 +379,35 @@ def run_warmstart(args):
         "vs_baseline": None, "loss_first_last": [losses[0], losses[-1]], **res}
 
 
+def run_converge(args):
+    """The 1600x640 channel time-marched from its initial condition until the
+    L-inf residual is <= 1e-8 (evaluated every 50 steps) or --max-steps; the
+    reference's CPU time for the same number of steps is extrapolated from a
+    bounded sample of its per-step time, and labelled as such."""
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    case = _case()
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision=args.precision)
+    res = solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=args.max_steps,
+                     residual_tol=1e-8, residual_every=50)
+    solver.close()
+    secs = res.device_ms * 1e-3
+    cpu = cpu_baseline_leg()
+    cpu_secs = CELLS * res.steps / cpu["value"] if cpu.get("value") else None
+    return {
+        "metric": "time to L-inf residual 1e-8, 1600x640 channel", "value": secs, "unit": "s",
+        "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "vs_baseline": None,
+        "data": "synthetic", "config": workload_config(),
+        "steps": res.steps, "converged": bool(res.converged), "residual": res.residual,
+        "status": res.status, "t": res.t,
+        "cell_updates_per_s": CELLS * res.steps / secs,
+        "cpu_baseline": cpu,
+        "cpu_seconds_extrapolated": cpu_secs,
+        "cpu_extrapolation": "reference CPU per-step time on a bounded sample x the GPU's steps",
+    }
+
+
 def run_serve(args):
     """The serving mix, bounded: a large converging-diverging
     channel warm-started from the surrogate (coarse prediction remapped on
@@ -593,7 +624,7 @@ def main():
     if args.workload != "plain":
         if rank == 0:
             runner = {"warmstart": run_warmstart, "surrogate": run_surrogate,
-                      "serve": run_serve}[args.workload]
+                      "serve": run_serve, "converge": run_converge}[args.workload]
             line = runner(args)
             print(json.dumps(line))
         return
