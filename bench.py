@@ -75,9 +75,13 @@ def parse():
 def workload_config():
     return {"workload": "plain FP64 LF time step, straight coaxial channel 1600x640",
             "L_max": L_MAX, "M_max": M_MAX, "cells_per_step": CELLS, "cfl": 0.4,
-            "adaptive_dt": True, "precision": "fast", "geometry": "r1=0.2, r2=0.8",
+            "adaptive_dt": True, "geometry": "r1=0.2, r2=0.8",
             "l2": "per-step working set 138 MB (8 planes read + 8 written) > 126 MB L2, no flush",
             "parallelism": "replicas"}
+
+
+PRECISION_OURS = "fast (reciprocal + FMA FP64; <= 1e-12 relative L-inf of the reference)"
+PRECISION_REF = "exact (the reference's own CPU build, IEEE FP64, no FMA contraction)"
 
 
 # ---------------------------------------------------------------- CPU side
@@ -86,25 +90,41 @@ def _case():
     return cases.channel_case(L=L_MAX, M=M_MAX)
 
 
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_child(spec: str) -> None:
     """Runs in a subprocess so OMP_NUM_THREADS applies: time the reference
-    CPU build (or the oracle port) on the workload and print JSON."""
+    CPU build (or the oracle port) on the workload and print JSON.  The
+    inputs come from oracle/channel.py (the reference's own geometry plugin
+    and ExpressionIC), so this process never loads the product library."""
     kind, steps, warmup = spec.split(":")
     steps, warmup = int(steps), int(warmup)
-    from oracle import bind
-    case = _case()
-    be = bind.Ref(case.oracle_dict()) if kind == "reference" else bind.Port(case.oracle_dict())
-    cfg = case.cfg
-    dt = cfg.dt
-    for _ in range(warmup):
+    from oracle import bind, channel
+    case = channel.channel_case(L_MAX, M_MAX)
+    be = bind.Ref(case) if kind == "reference" else bind.Port(case)
+    d = channel.DRIVER
+    dt = d["dt0"]
+
+    def step(dt):
         be.advance(dt)
-        dt = be.compute_dt(cfg.cfl_number, cfg.dt_growth_factor, cfg.dt_min, cfg.dt_max, dt)
+        return be.compute_dt(d["cfl"], d["growth"], d["dt_min"], d["dt_max"], dt)
+
+    for _ in range(warmup):
+        dt = step(dt)
     t0 = time.perf_counter()
     per = []
     for _ in range(steps):
         s0 = time.perf_counter()
-        be.advance(dt)
-        dt = be.compute_dt(cfg.cfl_number, cfg.dt_growth_factor, cfg.dt_min, cfg.dt_max, dt)
+        dt = step(dt)
         per.append(time.perf_counter() - s0)
     el = time.perf_counter() - t0
     print(json.dumps({"seconds": el, "steps": steps, "per_step": per}))
@@ -135,6 +155,7 @@ def cpu_baseline_leg() -> dict:
     res = run_cpu(kind, steps, 1, threads)
     value = CELLS * res["steps"] / res["seconds"]
     return {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+            "cpu_model": cpu_model(), "precision": PRECISION_REF,
             "sample": f"{res['steps']} time steps of the 1600x640 channel "
                       f"(OMP_NUM_THREADS={threads}, OMP_PROC_BIND=close)"}
 
@@ -200,60 +221,64 @@ def measured_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per interior-kernel launch from the committed ncu summary."""
-    p = ROOT / "profiles" / "lf_tma_kernel_1600x640.md"
-    if not p.exists():
-        return None
-    for line in p.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1])
-            except ValueError:
-                return None
-    return None
+def profiled_traffic(kernel: str = "lf_tma_kernel"):
+    """DRAM bytes per launch of `kernel` from one ncu capture (profiles/traffic.json)."""
+    p = ROOT / "profiles" / "traffic.json"
+    try:
+        d = json.loads(p.read_text())[kernel]
+        return float(d["dram_bytes_per_launch"]), d.get("note", "")
+    except (OSError, KeyError, ValueError, TypeError):
+        return None, "no ncu capture recorded"
 
 
 # ---------------------------------------------------------------- GPU side
 RESID_BYTES_PER_CELL = 128  # 8 new + 8 old conserved values read per interior cell
 
 
-def residual_cost(solver, dt, hbm_peak, steps=500):
-    """Device time of one L-inf residual evaluation in the graph loop: a run
-    evaluating it after every step minus a run without, per step."""
-    with_r = solver.run(T=1e300, dt=dt, adaptive=True, max_steps=steps,
-                        residual_tol=1e-300, residual_every=1)
-    without = solver.run(T=1e300, dt=with_r.dt, adaptive=True, max_steps=steps)
-    ms = (with_r.device_ms - without.device_ms) / steps
-    gbs = RESID_BYTES_PER_CELL * CELLS / (ms * 1e-3) / 1e9 if ms > 0 else None
-    return {"kernel": "residual_kernel", "ms": ms, "achieved": gbs, "unit": "GB/s",
-            "peak": hbm_peak, "frac": gbs / hbm_peak if gbs and hbm_peak else None,
-            "how": f"graph-loop device time with a residual after every step minus "
-                   f"without, {steps} steps each"}
+def graph_chunk(steps: int) -> int:
+    """Steps per captured CUDA graph for a timed run of `steps` steps: the
+    largest divisor of `steps` up to 100, so the run launches whole graphs
+    only (no launch runs past the last step); 100 when `steps` has no divisor
+    of at least 10 up to 100 (the last launch then ends in early exits)."""
+    if steps <= 100:
+        return max(steps, 1)
+    for d in range(100, 9, -1):
+        if steps % d == 0:
+            return d
+    return 100
 
 
 def run_ours(args, rank, world, local_rank):
+    import numpy as np
     import torch
     import __graft_entry__
     pkg = __graft_entry__.load_package()
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
+        import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", device_id=torch.device("cuda", local_rank))
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local_rank),
+                                timeout=datetime.timedelta(seconds=300))
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        tt = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
 
     case = _case()
     cfg = case.cfg
     solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
-    stream = torch.cuda.ExternalStream(solver.stream_handle())
+    per_graph = graph_chunk(args.steps)
 
-    # warm-up (includes the exact first step and the graph build)
-    # one graph of exactly --warmup steps, so no launch in the profile is an
-    # early exit of a graph that ran past the step limit
+    # warm-up: the exact first step, then W - 1 steps through the very graph
+    # (same steps per launch, same flags) that the timed run replays, so the
+    # capture and instantiation happen here and not inside the timed region
     w = max(args.warmup, 1)
-    solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=w, steps_per_graph=w)
-    _, step0 = solver.time()
-    dt_now = solver.ComputeDt(cfg.dt)
+    wres = solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=w, steps_per_graph=per_graph)
+    assert wres.steps == w, wres
 
     uuid = None
     try:
@@ -266,59 +291,55 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    res = solver.run(T=1e300, dt=dt_now, adaptive=True, max_steps=args.steps)
-    e1.record(stream)
-    e1.synchronize()
+    # K steps as K / per_graph launches of the captured graph, back to back;
+    # device_ms is CUDA events on the solver's stream around exactly them
+    res = solver.run(T=1e300, dt=wres.dt, adaptive=True, max_steps=args.steps,
+                     steps_per_graph=per_graph)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    t_max = ms
-    if dist:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
     assert res.steps == args.steps, res
+    t_max = max_over_ranks(res.device_ms)
 
-    # roofline of the dominant kernel: live CUDA events per launch
-    int_ms, bc_ms = solver.profile_kernels(50, res.dt)
-    resid = residual_cost(solver, res.dt, hbm_peak=measured_hbm()[0])
+    # per-launch device time of the dominant kernel and of the residual pass:
+    # back-to-back launches between two events on the solver's stream
     hbm, hbm_src = measured_hbm()
+    int_ms = solver.profile_kernel("interior", 30, res.dt)
+    resid_ms = solver.profile_kernel("residual", 30, res.dt)
     achieved = ALG_BYTES_PER_CELL * CELLS / (int_ms * 1e-3) / 1e9
-    traffic = profiled_traffic()
+    resid_gbs = RESID_BYTES_PER_CELL * CELLS / (resid_ms * 1e-3) / 1e9
+    traffic, traffic_note = profiled_traffic("lf_tma_kernel")
 
-    # end to end through the C ABI with host buffers: the reference driver's
-    # per-step pattern (Advance, then ComputeDt back on the host), with the
-    # initial state uploaded from and the final state read into pinned memory
-    import numpy as np
-    lib = solver.lib
+    # end to end through the public API with host buffers: the initial
+    # physical planes uploaded from pinned memory, the reference driver's
+    # per-step pattern (Advance(dt), then ComputeDt back on the host: 8 bytes
+    # each way per step), and the final physical planes read back into pinned
+    # memory (IOManager's output, mpd_snapshot_async); every phase timed
     shape = (10,) + solver.shape
     h_in = torch.from_numpy(np.ascontiguousarray(case.phys)).pin_memory()
-    h_out = torch.empty((8,) + solver.shape, dtype=torch.float64).pin_memory()
+    h_out = torch.empty(shape, dtype=torch.float64).pin_memory()
     n_e2e = args.steps
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     solver.set_physical(h_in.numpy())
+    t1 = time.perf_counter()
     dt = cfg.dt
     for _ in range(n_e2e):
         solver.Advance(dt)
         dt = solver.ComputeDt(dt)
-    for k in range(8):
-        lib.mpd_download(solver.h, k, ctypes.cast(ctypes.c_void_p(h_out[k].data_ptr()),
-                                                  pkg._native.DP))
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        tt = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    t2 = time.perf_counter()
+    solver.snapshot_async(h_out)
+    solver.snapshot_wait()
+    t3 = time.perf_counter()
+    e2e_s = max_over_ranks(t3 - t0)
+    phases = {"upload_ms": 1e3 * (t1 - t0), "steps_ms": 1e3 * (t2 - t1),
+              "download_ms": 1e3 * (t3 - t2)}
     plane = solver.shape[0] * solver.shape[1] * 8
     h2d = (10 * plane + 8 * n_e2e) / n_e2e          # IC planes + dt per step
-    d2h = (8 * plane) / n_e2e + 8                   # final state + dt per step
+    d2h = (10 * plane + 8 * n_e2e) / n_e2e          # output planes + dt per step
     solver.close()
 
     line = None
@@ -336,15 +357,31 @@ def run_ours(args, rank, world, local_rank):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "precision": PRECISION_OURS,
             "config": workload_config(),
+            "timing": f"CUDA events on the solver stream around {args.steps // per_graph} "
+                      f"back-to-back launches of one captured graph of {per_graph} steps "
+                      f"(2 kernels per step), built during warm-up; max over ranks",
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
+                         "traffic_note": traffic_note,
                          "kernel": "lf_tma_kernel", "kernel_ms": int_ms,
-                         "bc_kernel_ms": bc_ms, "peak_source": hbm_src},
-            "residual_kernel": resid,
+                         "alg_bytes_per_launch": ALG_BYTES_PER_CELL * CELLS,
+                         "kernel_timing": "30 back-to-back launches between two CUDA events",
+                         "peak_source": hbm_src},
+            "residual_kernel": {"kernel": "residual_kernel", "ms": resid_ms,
+                                "achieved": resid_gbs, "unit": "GB/s", "peak": hbm,
+                                "frac": resid_gbs / hbm,
+                                "alg_bytes_per_launch": RESID_BYTES_PER_CELL * CELLS,
+                                "how": "30 back-to-back launches between two CUDA events"},
             "cpu_baseline": cpu,
             "e2e": {"value": world * CELLS * n_e2e / e2e_s, "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": n_e2e, "phases_ms_rank0": phases,
+                    "how": "set_physical from pinned host planes, K x (Advance, ComputeDt), "
+                           "snapshot of the 10 physical planes into pinned host memory; "
+                           "host wall clock, max over ranks; upload and download amortised "
+                           "over the K steps"},
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
         }
@@ -582,6 +619,11 @@ def run_profile(args):
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the step (oracle/_ref: its
+    translation units compiled unchanged; the oracle port if that build is
+    absent) on all host threads, same workload, metric and config as our arm.
+    Its inputs come from oracle/channel.py, so no process of this arm loads
+    the product library.  Under torchrun only rank 0 runs."""
     if rank != 0:
         return None
     threads = os.cpu_count() or 1
@@ -589,7 +631,7 @@ def run_reference(args, rank, world):
     probe = run_cpu(kind, 1, 0, threads)
     per = max(probe["seconds"], 1e-6)
     steps = max(1, min(args.steps, int(150.0 / per)))   # bounded: a few minutes at most
-    warm = min(args.warmup, 3)
+    warm = max(0, min(args.warmup, int(30.0 / per)))
     res = run_cpu(kind, steps, warm, threads)
     value = CELLS * res["steps"] / res["seconds"]
     return {
@@ -597,9 +639,12 @@ def run_reference(args, rank, world):
         "n_gpus": world, "steps": res["steps"], "warmup": warm,
         "ms_per_step": 1e3 * res["seconds"] / res["steps"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "precision": PRECISION_REF,
         "config": workload_config(),
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": kind,
-                         "sample": f"{res['steps']} of the requested {args.steps} time steps"},
+                         "cpu_model": cpu_model(),
+                         "sample": f"{res['steps']} of the requested {args.steps} time steps "
+                                   f"(OMP_NUM_THREADS={threads}, OMP_PROC_BIND=close)"},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -217,6 +217,18 @@ int mpd_device_bytes(mpd_solver *s, size_t *bytes);
  * the interior kernel (out_ms[0]) and the boundary kernel (out_ms[1]). */
 int mpd_profile_kernels(mpd_solver *s, int steps, double dt, double out_ms[2]);
 
+/* Measurement support (new; no reference counterpart): the mean device time
+ * in ms of one launch of a step kernel, from `launches` back-to-back launches
+ * between two events on the handle's stream, with nothing else between them.
+ * MPD_KERNEL_INTERIOR: the interior kernel of the handle's precision at time
+ * step dt; every launch recomputes the next step's interior cells from the
+ * current state (the step counter does not advance; the state stays valid).
+ * MPD_KERNEL_RESIDUAL: the L-inf residual pass over the current and previous
+ * state.  Needs a handle that has taken at least one step. */
+#define MPD_KERNEL_INTERIOR 0
+#define MPD_KERNEL_RESIDUAL 1
+int mpd_profile_kernel(mpd_solver *s, int which, int launches, double dt, double *ms);
+
 /* ---- conserved integrals without allocating ----------------------------------- */
 /* No counterpart in the reference.  For callers that cannot let a library call
  * cudaMalloc: a host whose framework owns every byte of device memory through
@@ -230,12 +242,16 @@ int mpd_profile_kernels(mpd_solver *s, int steps, double dt, double out_ms[2]);
  *   d_out7 receives the 7 sums (device memory).
  * Work is enqueued on `stream` (a cudaStream_t; NULL = the default stream)
  * and not waited for.  Its only scratch is a fixed device array of 8192 rows
- * x 7 doubles (458,752 bytes) that every GPU loading the library keeps until
- * the process exits; L_max > 8192 is rejected with MPD_ERR_INVALID.  The
- * first call on a device looks up that array's device address, so make it
- * before any stream capture.  All calls share the one array and each rewrites
- * the rows it uses: calls whose work overlaps on the GPU race.  Calls no
- * cudaMalloc, cudaFree or allocating library routine. */
+ * x 7 doubles (458,752 bytes per GPU, kept until the process exits);
+ * L_max > 8192 is rejected with MPD_ERR_INVALID.  Under CUDA's lazy module
+ * loading (the default) that array is created when the first call on a
+ * device loads the library's module, so make a first (warm-up) call on each
+ * device before the caller's pool reserves the device's memory, and before
+ * any stream capture.  Every call looks the array's address up in the
+ * current context (nothing is cached across contexts or device resets).  All
+ * calls share the one array and each rewrites the rows it uses: calls whose
+ * work overlaps on the GPU race.  Calls no cudaMalloc, cudaFree or allocating
+ * library routine. */
 int mpd_integrals_noalloc(const double *d_u, size_t plane_stride, int pitch, int L_max,
                           int M_max, const double *d_dr, double dz, double *d_out7,
                           void *stream);

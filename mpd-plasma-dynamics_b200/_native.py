@@ -34,6 +34,7 @@ FACE_L_LO, FACE_L_HI, FACE_M_LO, FACE_M_HI = 0, 1, 2, 3
 NEUMANN, DIRICHLET, EXPRESSION, AXIS_LF = 0, 1, 2, 3
 ENGINE_AUTO, ENGINE_GRAPH, ENGINE_PERSISTENT = 0, 1, 2
 PRECISION_EXACT, PRECISION_FAST = 0, 1
+KERNEL_INTERIOR, KERNEL_RESIDUAL = 0, 1
 PHYS_FIELDS = ("rho", "v_z", "v_r", "v_phi", "e", "p", "P", "H_z", "H_r", "H_phi")
 
 DP = C.POINTER(C.c_double)
@@ -127,6 +128,7 @@ SIGNATURES = [
     ("mpd_get_stream", C.c_int, [_VP, C.POINTER(_VP)]),
     ("mpd_device_bytes", C.c_int, [_VP, C.POINTER(C.c_size_t)]),
     ("mpd_profile_kernels", C.c_int, [_VP, C.c_int, C.c_double, DP]),
+    ("mpd_profile_kernel", C.c_int, [_VP, C.c_int, C.c_int, C.c_double, DP]),
     ("mpd_integrals_noalloc", C.c_int, [_VP, C.c_size_t, C.c_int, C.c_int, C.c_int, _VP, C.c_double,
                                         _VP, _VP]),
     ("mpd_batch_create", C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(_VP)]),

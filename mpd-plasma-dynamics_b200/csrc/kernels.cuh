@@ -494,10 +494,12 @@ struct ResidAcc {
     }
 };
 
+// force: evaluate even when this step's residual is already known (timing).
 __global__ void __launch_bounds__(256) residual_kernel(Geo g, const double *buf0,
-                                                       const double *buf1, DevState *st) {
+                                                       const double *buf1, DevState *st,
+                                                       int force) {
     const long long step = st->step;
-    if (step == 0 || st->resid_step == step) return;
+    if (step == 0 || (!force && st->resid_step == step)) return;
     const double *un = (step & 1) ? buf1 : buf0;
     const double *uo = (step & 1) ? buf0 : buf1;
     ResidAcc acc;

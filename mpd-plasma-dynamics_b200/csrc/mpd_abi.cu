@@ -111,6 +111,8 @@ struct mpd_solver {
     unsigned long long *red = nullptr;
     mpd::DevState *st = nullptr;
     mpd::DevState *h_st = nullptr;  // pinned mirror
+    mpd::DevState *h_ring = nullptr;  // pinned: the state after each in-flight graph launch
+    cudaEvent_t ev_ring[2] = {nullptr, nullptr};
     mpd::HostMirror *hm = nullptr;   // mapped pinned: the controller's per-step outputs
     cudaEvent_t ev_sync = nullptr;   // completion of the enqueued work, for hm
     mpd::SegDesc *d_seg = nullptr;
@@ -176,6 +178,9 @@ void FreeAll(mpd_solver *s) {
     cudaFree(s->d_code);
     cudaFree(s->d_consts);
     if (s->h_st) cudaFreeHost(s->h_st);
+    if (s->h_ring) cudaFreeHost(s->h_ring);
+    for (cudaEvent_t e : s->ev_ring)
+        if (e) cudaEventDestroy(e);
     if (s->hm) cudaFreeHost(s->hm);
     if (s->ev_sync) cudaEventDestroy(s->ev_sync);
     if (s->ev0) cudaEventDestroy(s->ev0);
@@ -301,7 +306,7 @@ int EnqueueStep(mpd_solver *s, bool first, bool use_state_dt, double dt, bool wi
         MPD_CK(cudaGetLastError());
     }
     if (with_residual) {
-        mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(g, s->buf[0], s->buf[1], s->st);
+        mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(g, s->buf[0], s->buf[1], s->st, 0);
         MPD_CK(cudaGetLastError());
     }
     return MPD_OK;
@@ -445,6 +450,10 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     STEP(DevAlloc(s, &s->red, 4));
     STEP(DevAlloc(s, &s->st, 1));
     if (cudaMallocHost(reinterpret_cast<void **>(&s->h_st), sizeof(mpd::DevState)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void **>(&s->h_ring), 2 * sizeof(mpd::DevState)) !=
+            cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_ring[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_ring[1], cudaEventDisableTiming) != cudaSuccess ||
         cudaHostAlloc(reinterpret_cast<void **>(&s->hm), sizeof(mpd::HostMirror),
                       cudaHostAllocMapped) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_sync, cudaEventDisableTiming) != cudaSuccess) {
@@ -562,7 +571,7 @@ static int FinishRun(mpd_solver *s, long long step0, mpd_run_stats *stats) {
     MPD_CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     // the residual of the final state, when the loop stopped between checks
     if (!h.resid_valid && h.step > 0) {
-        mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st);
+        mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st, 0);
         MPD_CK(cudaGetLastError());
     }
     rc = SyncState(s);
@@ -727,18 +736,57 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
         per_graph = (per_graph / p->residual_every + 1) * p->residual_every;
     rc = BuildGraph(s, per_graph, with_check, want_ws, p->residual_every);
     if (rc != MPD_OK) return rc;
-    long long last_step = -1;
-    for (;;) {
-        MPD_CK(cudaMemcpyAsync(s->h_st, s->st, sizeof(mpd::DevState), cudaMemcpyDeviceToHost,
-                               s->stream));
-        MPD_CK(cudaStreamSynchronize(s->stream));
-        if (h.wait_fail)
-            return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
-        if (h.done) break;
-        if (h.step == last_step)  // a launch that advanced nothing: stop, don't spin
-            return Fail(MPD_ERR_TIMEOUT, "run loop made no progress");
-        last_step = h.step;
+    // Two graph launches in flight: after each launch the controller state is
+    // copied into a pinned slot, and the host reads the older slot while the
+    // newer launch runs, so the device never waits for the host between
+    // launches.  Every stop criterion is evaluated on the device (a launch
+    // after the stop exits at once); launches are capped at the step budget,
+    // so a fixed-step run queues no launch past its last step.
+    const long long first_taken = (!h.done && s->host_step == 0) ? 1 : 0;
+    const long long budget = p->max_steps - first_taken;
+    const long long cap = h.done || budget <= 0 ? 0 : (budget + per_graph - 1) / per_graph;
+    long long launched = 0;
+    int pending = 0;
+    auto launch = [&](int slot) -> int {
         MPD_CK(cudaGraphLaunch(s->graph, s->stream));
+        MPD_CK(cudaMemcpyAsync(&s->h_ring[slot], s->st, sizeof(mpd::DevState),
+                               cudaMemcpyDeviceToHost, s->stream));
+        MPD_CK(cudaEventRecord(s->ev_ring[slot], s->stream));
+        ++launched;
+        ++pending;
+        return MPD_OK;
+    };
+    for (int slot = 0; slot < 2 && launched < cap; ++slot) {
+        rc = launch(slot);
+        if (rc != MPD_OK) return rc;
+    }
+    long long last_step = -1;
+    bool stopped = h.done != 0;
+    for (int slot = 0; pending > 0; slot ^= 1) {
+        MPD_CK(cudaEventSynchronize(s->ev_ring[slot]));
+        --pending;
+        const mpd::DevState &r = s->h_ring[slot];
+        if (r.wait_fail) {
+            MPD_CK(cudaStreamSynchronize(s->stream));
+            return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
+        }
+        if (r.done) {
+            stopped = true;
+            break;  // a launch still in flight exits at once; FinishRun waits for it
+        }
+        if (r.step == last_step) {  // a launch that advanced nothing: stop, don't spin
+            MPD_CK(cudaStreamSynchronize(s->stream));
+            return Fail(MPD_ERR_TIMEOUT, "run loop made no progress");
+        }
+        last_step = r.step;
+        if (launched < cap) {
+            rc = launch(slot);
+            if (rc != MPD_OK) return rc;
+        }
+    }
+    if (!stopped) {
+        MPD_CK(cudaStreamSynchronize(s->stream));
+        return Fail(MPD_ERR_TIMEOUT, "run loop ended before the device controller stopped");
     }
     return FinishRun(s, step0, stats);
 }
@@ -874,7 +922,7 @@ int mpd_residual(mpd_solver *s, double *out) {
     int rc = CheckHandle(s);
     if (rc != MPD_OK) return rc;
     if (!out) return Fail(MPD_ERR_INVALID, "out is NULL");
-    mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st);
+    mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st, 0);
     MPD_CK(cudaGetLastError());
     rc = SyncState(s);
     if (rc != MPD_OK) return rc;
@@ -1088,6 +1136,41 @@ int mpd_profile_kernels(mpd_solver *s, int steps, double dt, double out_ms[2]) {
     out_ms[0] = tot[0] / steps;
     out_ms[1] = tot[1] / steps;
     return MPD_OK;
+}
+
+int mpd_profile_kernel(mpd_solver *s, int which, int launches, double dt, double *ms) {
+    int rc = CheckHandle(s);
+    if (rc != MPD_OK) return rc;
+    if (launches <= 0 || !ms || (which != MPD_KERNEL_INTERIOR && which != MPD_KERNEL_RESIDUAL))
+        return Fail(MPD_ERR_INVALID, "bad profile request");
+    rc = SyncState(s);
+    if (rc != MPD_OK) return rc;
+    if (s->h_st->step == 0)
+        return Fail(MPD_ERR_INVALID, "profile a kernel after the first step");
+    MPD_CK(cudaEventRecord(s->ev0, s->stream));
+    for (int i = 0; i < launches && rc == MPD_OK; ++i) {
+        if (which == MPD_KERNEL_INTERIOR) {
+            rc = LaunchInterior(s, false, false, dt, true);
+        } else {
+            mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0],
+                                                                         s->buf[1], s->st, 1);
+            MPD_CK(cudaGetLastError());
+        }
+    }
+    if (rc != MPD_OK) return rc;
+    MPD_CK(cudaEventRecord(s->ev1, s->stream));
+    MPD_CK(cudaEventSynchronize(s->ev1));
+    float t = 0.f;
+    MPD_CK(cudaEventElapsedTime(&t, s->ev0, s->ev1));
+    *ms = static_cast<double>(t) / launches;
+    // the interior launches folded this dt's wave speed into the step's
+    // accumulator: clear it, so the next step's controller sees only its own
+    if (which == MPD_KERNEL_INTERIOR) {
+        MPD_CK(cudaMemsetAsync(&s->st->ws_acc, 0, sizeof(unsigned long long), s->stream));
+        MPD_CK(cudaMemsetAsync(&s->st->nf_acc, 0, sizeof(unsigned int), s->stream));
+        MPD_CK(cudaStreamSynchronize(s->stream));
+    }
+    return SyncState(s);
 }
 
 int mpd_device_bytes(mpd_solver *s, size_t *bytes) {

@@ -8,11 +8,12 @@
 // memory budget out and must not see new allocations appear.  For them this
 // variant of Verification::ComputeIntegrals keeps its only scratch — one
 // partial sum per grid row — in a fixed file-scope device array instead of
-// the handle's cudaMalloc'd buffer.  Every GPU that loads the library holds
-// that array until the process exits.
+// the handle's cudaMalloc'd buffer.  The array belongs to this file's module:
+// under CUDA's lazy module loading (the default) a device gets its copy when
+// the first call on it loads the module, and keeps it until the process
+// exits; with eager loading, when the library is loaded.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/mpd_b200.h"
@@ -24,16 +25,10 @@ void SetLastError(const std::string &msg);
 namespace {
 
 constexpr int kNoAllocMaxRows = 8192;   // grid rows L_max the scratch can hold
-constexpr int kNoAllocMaxDevices = 64;
 
 // One partial sum per row and integral (7 doubles per row, 458,752 bytes).
 static __device__ __align__(256) double g_row_partials[kNoAllocMaxRows * 7];
 
-// Device address of g_row_partials, looked up once per device.  In host
-// code the symbol names a host-side stand-in, not device memory, so kernels
-// are given this address instead.
-double *g_partials_ptr[kNoAllocMaxDevices] = {};
-std::mutex g_setup_mutex;
 
 // Row l = 1 + blockIdx.x: the 7 sums of Verification::ComputeIntegrals
 // (src/verification.cpp:16-45) over m = 1..M+1, in order mass, mom_z, mom_r,
@@ -77,30 +72,21 @@ __global__ void noalloc_sum_kernel(const double *partials, int rows, double *out
     out7[threadIdx.x] = s;
 }
 
-// Once per device, with that device current: resolve the scratch address.
-int ScratchForCurrentDevice(double **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        mpd::SetLastError(std::string("mpd_integrals_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+// The device address of g_row_partials in the current context.  In host code
+// the symbol names a host-side stand-in, not device memory, so kernels are
+// given this address instead.  It is looked up on every call rather than
+// cached: a cached address would outlive a device reset or belong to another
+// context (a framework may make a non-primary context current), and the
+// lookup itself allocates nothing once the module is loaded.
+int ScratchForCurrentContext(double **out) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_row_partials);
+    if (e != cudaSuccess || !p) {
+        mpd::SetLastError(std::string("mpd_integrals_noalloc: cudaGetSymbolAddress: ") +
+                          cudaGetErrorString(e));
         return MPD_ERR_CUDA;
     }
-    if (dev < 0 || dev >= kNoAllocMaxDevices) {
-        mpd::SetLastError("mpd_integrals_noalloc: device index out of range");
-        return MPD_ERR_INVALID;
-    }
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials_ptr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_row_partials);
-        if (e != cudaSuccess || !p) {
-            mpd::SetLastError(std::string("mpd_integrals_noalloc: cudaGetSymbolAddress: ") +
-                              cudaGetErrorString(e));
-            return MPD_ERR_CUDA;
-        }
-        g_partials_ptr[dev] = static_cast<double *>(p);
-    }
-    *out = g_partials_ptr[dev];
+    *out = static_cast<double *>(p);
     return MPD_OK;
 }
 
@@ -121,7 +107,7 @@ extern "C" int mpd_integrals_noalloc(const double *d_u, size_t plane_stride, int
         return MPD_ERR_INVALID;
     }
     double *partials = nullptr;
-    const int rc = ScratchForCurrentDevice(&partials);
+    const int rc = ScratchForCurrentContext(&partials);
     if (rc != MPD_OK) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // every row's partials are rewritten before they are summed: nothing in

@@ -213,6 +213,19 @@ class GpuSolver:
     def physical(self) -> np.ndarray:
         return np.stack([self.download(8 + k) for k in range(10)])
 
+    def snapshot_async(self, pinned_phys10) -> None:
+        """IOManager's output planes (src/io_manager.cpp:68-77): the 10 physical
+        planes of the current state, copied on a side stream into caller-owned
+        pinned host memory of shape (10, L+2, M+3) (a pinned torch tensor, or
+        any object with ``data_ptr()``); stepping may continue meanwhile.  The
+        buffer is complete after ``snapshot_wait``."""
+        ptr = pinned_phys10.data_ptr() if hasattr(pinned_phys10, "data_ptr") else \
+            pinned_phys10.ctypes.data
+        self._call("mpd_snapshot_async", C.cast(C.c_void_p(ptr), N.DP))
+
+    def snapshot_wait(self) -> None:
+        self._call("mpd_snapshot_wait")
+
     def set_physical(self, phys10: np.ndarray) -> None:
         a = np.ascontiguousarray(phys10, dtype=np.float64)
         self._call("mpd_set_physical", _dp(a))
@@ -227,6 +240,14 @@ class GpuSolver:
         out = np.zeros(2)
         self._call("mpd_profile_kernels", int(steps), float(dt), _dp(out))
         return float(out[0]), float(out[1])
+
+    def profile_kernel(self, which: str, launches: int, dt: float) -> float:
+        """Mean device ms of one launch of the interior kernel ("interior")
+        or the residual pass ("residual"), from back-to-back launches."""
+        out = np.zeros(1)
+        k = {"interior": N.KERNEL_INTERIOR, "residual": N.KERNEL_RESIDUAL}[which]
+        self._call("mpd_profile_kernel", k, int(launches), float(dt), _dp(out))
+        return float(out[0])
 
     def device_bytes(self) -> int:
         b = C.c_size_t()

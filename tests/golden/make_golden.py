@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import os
 import pathlib
 import subprocess
 import sys
@@ -86,7 +87,8 @@ def record(name, cfg, use_ref_geometry, checkpoints, digest_only=False):
 
 
 def main():
-    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref"], check=True)
+    ref = os.environ.get("MPD_REFERENCE", "/root/reference")  # the reference source tree
+    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), f"REF={ref}", "ref"], check=True)
     record("channel_sine_24x12", cases.channel_config(L=24, M=12, a=0.1), False, [1, 10, 100])
     record("reference_default_40x20", cases.reference_default_config(L=40, M=20), True,
            [1, 10, 60])

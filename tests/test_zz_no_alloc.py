@@ -47,12 +47,17 @@ def test_integrals_noalloc_matches_mpd_integrals_twice():
     out_a = torch.zeros(7, dtype=torch.float64, device="cuda")
     out_b = torch.zeros(7, dtype=torch.float64, device="cuda")
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    free = []
     for cons, out in ((cons_a, out_a), (cons_b, out_b)):   # two calls in a row
         rc = lib.mpd_integrals_noalloc(C.c_void_p(cons.data_ptr()), rows * cols, cols, cfg.L_max,
                                        cfg.M_max, C.c_void_p(dr.data_ptr()), cfg.dz,
                                        C.c_void_p(out.data_ptr()), stream)
         assert rc == N.MPD_OK, lib.mpd_last_error()
-    torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info()[0])
+    # the first call may load the library's module (lazy loading creates the
+    # fixed array then); the second must not change the device's free memory
+    assert free[1] == free[0], free
     np.testing.assert_allclose(out_a.cpu().numpy(), want_a, rtol=RTOL, atol=0)
     np.testing.assert_allclose(out_b.cpu().numpy(), want_b, rtol=RTOL, atol=0)
 
