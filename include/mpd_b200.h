@@ -126,6 +126,27 @@ int mpd_advance(mpd_solver *s, double dt);
 #define MPD_ENGINE_GRAPH 1
 #define MPD_ENGINE_PERSISTENT 2
 
+/* One report of the reference driver loop's periodic diagnostics
+ * (src/main.cpp:249-281), taken by mpd_run after every step whose count is a
+ * multiple of mpd_run_params.monitor_every (the reference: 1000). */
+typedef struct mpd_monitor_record {
+    long long step;        /* step count since the solver's initial state        */
+    double t;              /* simulated time after that step                     */
+    double dt;             /* dt of the next step (after the adaptive update)    */
+    double probe[5];       /* rho, v_z, v_phi, e, H_phi at the global cell
+                              (l 20, m 40) (src/main.cpp:196-197,258-270);
+                              0 when the grid has no such cell                   */
+    double integrals[7];   /* Verification::ComputeIntegrals, src/verification.cpp:16-45 */
+    double max_wave_speed; /* Diagnostics::MaxWaveSpeed of the state             */
+    double dt_cfl;         /* cfl_number * min(dz, dy) / (max_wave_speed + 1e-10) */
+    int cfl_warning;       /* dt > dt_cfl: Diagnostics::CheckCfl's warning
+                              condition (src/diagnostics.cpp:112-125)            */
+} mpd_monitor_record;
+
+/* Called by mpd_run on its own host thread with the stream idle; the record
+ * is valid only during the call. */
+typedef void (*mpd_monitor_fn)(const mpd_monitor_record *record, void *user);
+
 typedef struct mpd_run_params {
     double T;                   /* end time (use a huge value for step-limited runs) */
     double dt;                  /* initial dt (SimConfig::dt); <= 0: the CFL limit of
@@ -139,6 +160,12 @@ typedef struct mpd_run_params {
     long long max_steps;
     int steps_per_graph;          /* steps captured per CUDA graph launch (0 = auto) */
     int engine;                   /* MPD_ENGINE_AUTO / _GRAPH / _PERSISTENT           */
+    int monitor_every;            /* steps between monitor reports; 0 = none. Needs
+                                     the graph engine; the loop then stops at every
+                                     multiple of it, and the residual schedule
+                                     restarts there                                  */
+    mpd_monitor_fn monitor;       /* NULL = no reports                               */
+    void *monitor_user;           /* passed to monitor                               */
 } mpd_run_params;
 
 typedef struct mpd_run_stats {

@@ -63,6 +63,16 @@ class Geometry(C.Structure):
     _fields_ = [("r_inner", DP), ("r_outer", DP), ("dr_inner_dz", DP), ("dr_outer_dz", DP)]
 
 
+class MonitorRecord(C.Structure):
+    _fields_ = [("step", C.c_longlong), ("t", C.c_double), ("dt", C.c_double),
+                ("probe", C.c_double * 5), ("integrals", C.c_double * 7),
+                ("max_wave_speed", C.c_double), ("dt_cfl", C.c_double),
+                ("cfl_warning", C.c_int)]
+
+
+MonitorFn = C.CFUNCTYPE(None, C.POINTER(MonitorRecord), C.c_void_p)
+
+
 class RunParams(C.Structure):
     _fields_ = [("T", C.c_double), ("dt", C.c_double), ("adaptive", C.c_int),
                 ("cfl_number", C.c_double), ("dt_growth_factor", C.c_double),
@@ -70,7 +80,8 @@ class RunParams(C.Structure):
                 ("convergence_threshold", C.c_double), ("check_frequency", C.c_int),
                 ("residual_tol", C.c_double), ("residual_every", C.c_int),
                 ("max_steps", C.c_longlong), ("steps_per_graph", C.c_int),
-                ("engine", C.c_int)]
+                ("engine", C.c_int), ("monitor_every", C.c_int), ("monitor", MonitorFn),
+                ("monitor_user", C.c_void_p)]
 
 
 class RunStats(C.Structure):

@@ -64,7 +64,7 @@ int mpd_emu_create(const mpd_config *cfg, const mpd_geometry *geom, const double
     s->buf[0].assign(8 * ps, 0.0);
     s->buf[1].assign(8 * ps, 0.0);
     s->ic.assign(10 * ps, 0.0);
-    s->geo.assign(5 * static_cast<size_t>(s->rows), 0.0);
+    s->geo.assign(6 * static_cast<size_t>(s->rows), 0.0);
     for (int l = 0; l < s->rows; ++l) {
         s->geo[0 * s->rows + l] = geom->r_inner[l];
         s->geo[1 * s->rows + l] = geom->r_outer[l];
@@ -72,6 +72,7 @@ int mpd_emu_create(const mpd_config *cfg, const mpd_geometry *geom, const double
         s->geo[3 * s->rows + l] = geom->dr_outer_dz[l];
         const double R = geom->r_outer[l] - geom->r_inner[l];
         s->geo[4 * s->rows + l] = R / M;
+        s->geo[5 * s->rows + l] = 0.5 / s->geo[4 * s->rows + l];
     }
     mpd::Geo &g = s->g;
     g.L = L;
@@ -89,6 +90,7 @@ int mpd_emu_create(const mpd_config *cfg, const mpd_geometry *geom, const double
     g.drin = s->geo.data() + 2 * s->rows;
     g.drout = s->geo.data() + 3 * s->rows;
     g.dr = s->geo.data() + 4 * s->rows;
+    g.hdr = s->geo.data() + 5 * s->rows;
     for (int k = 0; k < 10; ++k)
         for (int l = 1; l <= L; ++l)
             for (int m = 1; m <= M + 1; ++m) s->ic[k * ps + g.ix(l, m)] = phys10[k * ps + g.ix(l, m)];

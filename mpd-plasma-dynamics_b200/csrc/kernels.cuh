@@ -504,31 +504,41 @@ __global__ void __launch_bounds__(256) residual_kernel(Geo g, const double *buf0
     const double *uo = (step & 1) ? buf0 : buf1;
     ResidAcc acc;
     acc.init();
-    // units of one row x 32 consecutive columns, one per warp at a time: a
-    // warp's loads are whole 256-byte row segments, and all 16 of a lane's
-    // loads are issued before any is used.  The old state is read with the
-    // streaming policy: the next step overwrites it; the new one stays in L2
-    // as that step's input.  (Measured on a B200 at 1600 x 640, in the graph
-    // loop: 95 us per evaluation with one thread per cell and a 64-bit key
-    // with a NaN test per value, 29 us so; runs of consecutive units per
-    // warp, or four blocks per SM at 64 registers, measured slower.)
-    const int W = g.M + 1;
-    const int nch = (W + 31) >> 5;
-    const int units = g.L * nch;
-    const int lane = threadIdx.x & 31;
-    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-    for (int u = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); u < units; u += nwarps) {
-        const int row = u / nch;
-        const int m = 1 + (u - row * nch) * 32 + lane;
-        if (m > W) continue;
-        const size_t i = g.ix(1 + row, m);
-        double a[8], b[8];
+    // Items of one row l in [1, L] x one pair of columns (2c, 2c + 1),
+    // c < (M + 3) / 2: columns 0 .. M+1, plus the ghost column M+2 when M is
+    // odd.  Ghost columns are zero in both buffers, so they leave every
+    // maximum unchanged.  A thread issues all 16 of an item's 16-byte loads
+    // (8 planes, new and old state) before using any; rows are 256-byte
+    // aligned (pitch a multiple of 32 doubles), so every pair is a 16-byte
+    // aligned load and a warp reads 512 contiguous bytes per plane.  The old
+    // state is read with the streaming policy (the next step overwrites it);
+    // the new one stays in L2 as that step's input.
+    const int ncp = (g.M + 3) >> 1;
+    const int items = g.L * ncp;
+    const int stride = (int)(gridDim.x * blockDim.x);
+    for (int it = (int)(blockIdx.x * blockDim.x + threadIdx.x); it < items; it += stride) {
+        const int row = it / ncp;
+        const int c = it - row * ncp;
+        const size_t i = g.ix(1 + row, 2 * c);
+        double2 a[8], b[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            a[k] = __ldg(un + (size_t)k * g.ps + i);
-            b[k] = __ldcs(uo + (size_t)k * g.ps + i);
+            a[k] = __ldg(reinterpret_cast<const double2 *>(un + (size_t)k * g.ps + i));
+            b[k] = __ldcs(reinterpret_cast<const double2 *>(uo + (size_t)k * g.ps + i));
         }
-        acc.fold(a, b);
+        double an[8], ao[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            an[k] = a[k].x;
+            ao[k] = b[k].x;
+        }
+        acc.fold(an, ao);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            an[k] = a[k].y;
+            ao[k] = b[k].y;
+        }
+        acc.fold(an, ao);
     }
     unsigned long long key[16];
     unsigned int nf;

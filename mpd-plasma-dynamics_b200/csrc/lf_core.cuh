@@ -64,6 +64,7 @@ struct Geo {
     size_t ps;  // plane stride (doubles)
     double dz, dy, gamma, beta, H_z0, r_0;
     const double *rin, *rout, *drin, *drout, *dr;  // per row l = 0..L+1
+    const double *hdr;  // 0.5 / dr per row (the fast interior's r-difference factor)
 
     MPD_HD size_t ix(int l, int m) const { return (size_t)l * (size_t)pitch + (size_t)m; }
     MPD_HD double r(int l, int m) const {

@@ -440,7 +440,7 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     STEP(DevAlloc(s, &s->buf[1], 8 * s->ps));
     STEP(DevAlloc(s, &s->ic, 10 * s->ps));
     if (s->with_prev) STEP(DevAlloc(s, &s->prev, 7 * s->ps));
-    STEP(DevAlloc(s, &s->geo, 5 * static_cast<size_t>(s->rows)));
+    STEP(DevAlloc(s, &s->geo, 6 * static_cast<size_t>(s->rows)));
     STEP(DevAlloc(s, &s->partials, static_cast<size_t>(kRedBlocks) * 8));
     s->len = mpd::line_len(s->L, s->M);
     STEP(DevAlloc(s, &s->cphys, static_cast<size_t>(mpd::kCentralLines) * 8 * s->len));
@@ -463,7 +463,7 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     std::memset(s->hm, 0, sizeof(mpd::HostMirror));
     // wall profiles + dr (Grid::Build: R = r_outer - r_inner, dr = R / M_max)
     {
-        std::vector<double> h(5 * static_cast<size_t>(s->rows));
+        std::vector<double> h(6 * static_cast<size_t>(s->rows));
         for (int l = 0; l < s->rows; ++l) {
             h[0 * s->rows + l] = geom->r_inner[l];
             h[1 * s->rows + l] = geom->r_outer[l];
@@ -471,6 +471,7 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
             h[3 * s->rows + l] = geom->dr_outer_dz[l];
             const double R = geom->r_outer[l] - geom->r_inner[l];
             h[4 * s->rows + l] = R / cfg->M_max;
+            h[5 * s->rows + l] = 0.5 / h[4 * s->rows + l];
         }
         if (cudaMemcpy(s->geo, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice) !=
             cudaSuccess) {
@@ -494,6 +495,7 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     g.drin = s->geo + 2 * s->rows;
     g.drout = s->geo + 3 * s->rows;
     g.dr = s->geo + 4 * s->rows;
+    g.hdr = s->geo + 5 * s->rows;
     {
         int sms = 0, per_sm = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess ||
@@ -612,6 +614,9 @@ static int CheckRunParams(const mpd_solver *s, const mpd_run_params *p) {
     if (p->max_steps <= 0) return Fail(MPD_ERR_INVALID, "max_steps must be positive");
     if (p->residual_every < 0 || p->residual_every > 4096)
         return Fail(MPD_ERR_INVALID, "residual_every must be in [0, 4096]");
+    if (p->monitor_every < 0) return Fail(MPD_ERR_INVALID, "monitor_every must be >= 0");
+    if (p->monitor && p->monitor_every > 0 && p->engine == MPD_ENGINE_PERSISTENT)
+        return Fail(MPD_ERR_INVALID, "monitor reports need the graph engine");
     return MPD_OK;
 }
 
@@ -638,6 +643,11 @@ static int PrepareRun(mpd_solver *s, const mpd_run_params *p, long long &step0) 
     h.dt_max = p->dt_max;
     h.T = p->T;
     h.max_steps = step0 + p->max_steps;
+    if (p->monitor && p->monitor_every > 0) {
+        // the loop stops at every multiple of monitor_every for a report
+        const long long next = (step0 / p->monitor_every + 1) * p->monitor_every;
+        if (next < h.max_steps) h.max_steps = next;
+    }
     h.resid_tol = p->residual_tol;
     h.resid_every = p->residual_every > 0 ? p->residual_every : 0;
     h.conv_thr = p->convergence_threshold;
@@ -678,6 +688,99 @@ static mpd::PersistArgs PersistArgsOf(const mpd_solver *s, int nstrips, int nban
     a.nsteps = nsteps;
     a.resid_base = resid_base;
     return a;
+}
+
+// Graph launches until the device controller stops, taking at most `budget`
+// steps.  Two launches are kept in flight: after each launch the controller
+// state is copied into a pinned slot, and the host reads the older slot while
+// the newer launch runs, so the device never waits for the host between
+// launches.  Every stop criterion is evaluated on the device (a launch after
+// the stop exits at once); launches are capped at the budget, so a fixed-step
+// run queues no launch past its last step.
+static int GraphLoop(mpd_solver *s, long long budget, int per_graph) {
+    const long long cap = budget <= 0 ? 0 : (budget + per_graph - 1) / per_graph;
+    if (cap == 0) return MPD_OK;
+    long long launched = 0;
+    int pending = 0;
+    auto launch = [&](int slot) -> int {
+        MPD_CK(cudaGraphLaunch(s->graph, s->stream));
+        MPD_CK(cudaMemcpyAsync(&s->h_ring[slot], s->st, sizeof(mpd::DevState),
+                               cudaMemcpyDeviceToHost, s->stream));
+        MPD_CK(cudaEventRecord(s->ev_ring[slot], s->stream));
+        ++launched;
+        ++pending;
+        return MPD_OK;
+    };
+    int rc = MPD_OK;
+    for (int slot = 0; slot < 2 && launched < cap; ++slot) {
+        rc = launch(slot);
+        if (rc != MPD_OK) return rc;
+    }
+    long long last_step = -1;
+    for (int slot = 0; pending > 0; slot ^= 1) {
+        MPD_CK(cudaEventSynchronize(s->ev_ring[slot]));
+        --pending;
+        const mpd::DevState &r = s->h_ring[slot];
+        if (r.wait_fail) {
+            MPD_CK(cudaStreamSynchronize(s->stream));
+            return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
+        }
+        if (r.done) return MPD_OK;  // a launch still in flight exits at once
+        if (r.step == last_step) {  // a launch that advanced nothing: stop, don't spin
+            MPD_CK(cudaStreamSynchronize(s->stream));
+            return Fail(MPD_ERR_TIMEOUT, "run loop made no progress");
+        }
+        last_step = r.step;
+        if (launched < cap) {
+            rc = launch(slot);
+            if (rc != MPD_OK) return rc;
+        }
+    }
+    MPD_CK(cudaStreamSynchronize(s->stream));
+    return Fail(MPD_ERR_TIMEOUT, "run loop ended before the device controller stopped");
+}
+
+// The driver loop's periodic report (src/main.cpp:249-281) of the current
+// state, handed to the run's monitor callback.  s->h_st is current.
+static int Monitor(mpd_solver *s, const mpd_run_params *p) {
+    const mpd::DevState h = *s->h_st;
+    mpd_monitor_record rec{};
+    rec.step = h.step;
+    rec.t = h.t;
+    rec.dt = h.dt;
+    double speed = 0.0;
+    if (h.ws_valid && h.step > 0) {
+        speed = h.last_ws;
+    } else {
+        MPD_CK(cudaMemsetAsync(s->red, 0, 2 * sizeof(unsigned long long), s->stream));
+        mpd::wave_speed_kernel<<<kRedBlocks, 256, 0, s->stream>>>(Bufs(s), s->red);
+        MPD_CK(cudaGetLastError());
+        unsigned long long key = 0;
+        MPD_CK(cudaMemcpyAsync(&key, s->red, sizeof(key), cudaMemcpyDeviceToHost, s->stream));
+        MPD_CK(cudaStreamSynchronize(s->stream));
+        std::memcpy(&speed, &key, sizeof(double));
+    }
+    // Diagnostics::CheckCfl (src/diagnostics.cpp:112-125)
+    const double dx = s->g.dz < s->g.dy ? s->g.dz : s->g.dy;
+    rec.max_wave_speed = speed;
+    rec.dt_cfl = p->cfl_number * dx / (speed + 1.0e-10);
+    rec.cfl_warning = h.dt > rec.dt_cfl ? 1 : 0;
+    // the checkpoint cell (global l 20, m 40) when the grid has it
+    constexpr int kProbeL = 20, kProbeM = 40;
+    if (kProbeL < s->L && kProbeM <= s->M) {
+        double q[10];
+        int rc = mpd_probe(s, kProbeL, kProbeM, q);
+        if (rc != MPD_OK) return rc;
+        rec.probe[0] = q[0];  // rho
+        rec.probe[1] = q[1];  // v_z
+        rec.probe[2] = q[3];  // v_phi
+        rec.probe[3] = q[4];  // e
+        rec.probe[4] = q[9];  // H_phi
+    }
+    int rc = mpd_integrals(s, rec.integrals);
+    if (rc != MPD_OK) return rc;
+    p->monitor(&rec, p->monitor_user);
+    return MPD_OK;
 }
 
 int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
@@ -726,9 +829,20 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
         }
         return FinishRun(s, step0, stats);
     }
+    const bool monitored = p->monitor && p->monitor_every > 0;
     // Steps per graph launch: a multiple of the residual interval, so that the
-    // residual is evaluated every residual_every steps.
+    // residual is evaluated every residual_every steps; with monitor reports,
+    // a divisor of monitor_every where the residual interval allows.
     int per_graph = p->steps_per_graph > 0 ? p->steps_per_graph : 100;
+    if (monitored && p->monitor_every % per_graph != 0) {
+        int a = per_graph, b = p->monitor_every;
+        while (b) {
+            const int r = a % b;
+            a = b;
+            b = r;
+        }
+        per_graph = a;
+    }
     if (with_check && p->check_frequency > 0 && per_graph % p->check_frequency != 0 &&
         p->check_frequency < per_graph)
         per_graph = (per_graph / p->check_frequency) * p->check_frequency;
@@ -736,57 +850,34 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
         per_graph = (per_graph / p->residual_every + 1) * p->residual_every;
     rc = BuildGraph(s, per_graph, with_check, want_ws, p->residual_every);
     if (rc != MPD_OK) return rc;
-    // Two graph launches in flight: after each launch the controller state is
-    // copied into a pinned slot, and the host reads the older slot while the
-    // newer launch runs, so the device never waits for the host between
-    // launches.  Every stop criterion is evaluated on the device (a launch
-    // after the stop exits at once); launches are capped at the step budget,
-    // so a fixed-step run queues no launch past its last step.
-    const long long first_taken = (!h.done && s->host_step == 0) ? 1 : 0;
-    const long long budget = p->max_steps - first_taken;
-    const long long cap = h.done || budget <= 0 ? 0 : (budget + per_graph - 1) / per_graph;
-    long long launched = 0;
-    int pending = 0;
-    auto launch = [&](int slot) -> int {
-        MPD_CK(cudaGraphLaunch(s->graph, s->stream));
-        MPD_CK(cudaMemcpyAsync(&s->h_ring[slot], s->st, sizeof(mpd::DevState),
-                               cudaMemcpyDeviceToHost, s->stream));
-        MPD_CK(cudaEventRecord(s->ev_ring[slot], s->stream));
-        ++launched;
-        ++pending;
-        return MPD_OK;
-    };
-    for (int slot = 0; slot < 2 && launched < cap; ++slot) {
-        rc = launch(slot);
+    long long taken_before = (!h.done && s->host_step == 0) ? 1 : 0;  // the exact first step
+    const long long end = step0 + p->max_steps;
+    for (;;) {
+        // steps this segment may take: to the controller's current stop
+        long long budget = h.max_steps - h.step - taken_before;
+        taken_before = 0;
+        rc = GraphLoop(s, h.done ? 0 : budget, per_graph);
         if (rc != MPD_OK) return rc;
-    }
-    long long last_step = -1;
-    bool stopped = h.done != 0;
-    for (int slot = 0; pending > 0; slot ^= 1) {
-        MPD_CK(cudaEventSynchronize(s->ev_ring[slot]));
-        --pending;
-        const mpd::DevState &r = s->h_ring[slot];
-        if (r.wait_fail) {
-            MPD_CK(cudaStreamSynchronize(s->stream));
-            return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
+        if (!monitored) break;
+        rc = SyncState(s);
+        if (rc != MPD_OK) return rc;
+        if (h.converged || h.nonfinite || !(h.t < h.T) || h.step >= end) {
+            if (h.step % p->monitor_every == 0 && h.step > step0) {
+                rc = Monitor(s, p);
+                if (rc != MPD_OK) return rc;
+            }
+            break;
         }
-        if (r.done) {
-            stopped = true;
-            break;  // a launch still in flight exits at once; FinishRun waits for it
-        }
-        if (r.step == last_step) {  // a launch that advanced nothing: stop, don't spin
-            MPD_CK(cudaStreamSynchronize(s->stream));
-            return Fail(MPD_ERR_TIMEOUT, "run loop made no progress");
-        }
-        last_step = r.step;
-        if (launched < cap) {
-            rc = launch(slot);
+        if (h.step % p->monitor_every == 0) {
+            rc = Monitor(s, p);
             if (rc != MPD_OK) return rc;
         }
-    }
-    if (!stopped) {
-        MPD_CK(cudaStreamSynchronize(s->stream));
-        return Fail(MPD_ERR_TIMEOUT, "run loop ended before the device controller stopped");
+        // next segment: to the next report or the end of the run
+        const long long next = (h.step / p->monitor_every + 1) * p->monitor_every;
+        h.max_steps = next < end ? next : end;
+        h.done = 0;
+        rc = PushState(s);
+        if (rc != MPD_OK) return rc;
     }
     return FinishRun(s, step0, stats);
 }

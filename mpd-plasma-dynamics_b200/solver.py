@@ -24,6 +24,42 @@ ENGINES = {"auto": N.ENGINE_AUTO, "graph": N.ENGINE_GRAPH, "persistent": N.ENGIN
 
 
 @dataclasses.dataclass
+class MonitorReport:
+    """One periodic report of the driver loop (src/main.cpp:249-281)."""
+    step: int
+    t: float
+    dt: float
+    probe: tuple        # rho, v_z, v_phi, e, H_phi at the global cell (l 20, m 40)
+    integrals: tuple    # Verification::ComputeIntegrals
+    max_wave_speed: float
+    dt_cfl: float
+    cfl_warning: bool   # Diagnostics::CheckCfl's warning condition
+
+    @classmethod
+    def from_record(cls, r) -> "MonitorReport":
+        return cls(r.step, r.t, r.dt, tuple(r.probe), tuple(r.integrals), r.max_wave_speed,
+                   r.dt_cfl, bool(r.cfl_warning))
+
+
+def reference_report(rep: MonitorReport, cfl_number: float, out=None) -> None:
+    """Print a report the way the reference's driver does: the CheckCfl warning
+    (src/diagnostics.cpp:112-125, only at multiples of 1000 steps), the
+    checkpoint line (src/main.cpp:268-270) and the integral table row
+    (Verification::PrintIntegrals, src/verification.cpp:59-66)."""
+    import sys
+    out = out or sys.stdout
+    if rep.cfl_warning and rep.step % 1000 == 0:
+        out.write(f"WARNING [step {rep.step}]: dt={rep.dt:.6e} exceeds CFL limit "
+                  f"dt_max={rep.dt_cfl:.6e} (max_speed={rep.max_wave_speed:.3f}, "
+                  f"CFL={rep.dt / rep.dt_cfl * cfl_number:.2f})\n")
+    p = rep.probe
+    out.write(f"{rep.t:<14.6f} {rep.dt:<14.6e} {p[0]:<14.6f} {p[1]:<14.6f} {p[2]:<14.6f} "
+              f"{p[3]:<14.6f} {p[4]:<14.6f}\n")
+    q = rep.integrals
+    out.write(f"  {rep.step:<8d}  {rep.t:<12.5f}  " + "  ".join(f"{v:<14.6e}" for v in q) + "\n")
+
+
+@dataclasses.dataclass
 class RunResult:
     steps: int
     t: float
@@ -112,7 +148,8 @@ class GpuSolver:
     def run(self, T: float = float("inf"), dt: float | None = None, adaptive: bool | None = None,
             max_steps: int = 1 << 40, residual_tol: float = 0.0, residual_every: int | None = None,
             convergence_threshold: float | None = None, check_frequency: int | None = None,
-            steps_per_graph: int = 0, engine: str = "auto") -> RunResult:
+            steps_per_graph: int = 0, engine: str = "auto", monitor=None,
+            monitor_every: int = 1000) -> RunResult:
         """Graph-resident driver loop (src/main.cpp:191-282).
 
         The L-inf residual (a separate pass over both state buffers) is
@@ -121,6 +158,10 @@ class GpuSolver:
         ``engine``: "graph" (two kernels per step from captured CUDA graphs),
         "persistent" (one cooperative launch for many steps; fast precision
         without convergence_threshold) or "auto" (graph); both give the same bits.
+        ``monitor``: a callable given a ``MonitorReport`` after every
+        ``monitor_every`` steps (the reference driver's 1000-step checkpoint,
+        integrals and CheckCfl; ``reference_report`` prints it the reference's
+        way); graph engine only.
         """
         cfg = self.cfg
         if residual_every is None:
@@ -139,8 +180,20 @@ class GpuSolver:
         p.max_steps = int(max_steps)
         p.steps_per_graph = steps_per_graph
         p.engine = ENGINES[engine]
+        errors = []
+        if monitor is not None:
+            def _cb(rec, _user):
+                try:
+                    monitor(MonitorReport.from_record(rec.contents))
+                except Exception as exc:  # noqa: BLE001 - re-raised after the run
+                    errors.append(exc)
+            cb = N.MonitorFn(_cb)
+            p.monitor = cb
+            p.monitor_every = int(monitor_every)
         st = N.RunStats()
         rc = self.lib.mpd_run(self.h, C.byref(p), C.byref(st))
+        if errors:
+            raise errors[0]
         if rc not in (N.MPD_OK, N.MPD_ERR_NONFINITE):
             N.check(rc, self.lib)
         return RunResult(st.steps, st.t, st.dt, st.residual, st.change, st.max_wave_speed,

@@ -96,3 +96,34 @@ def test_batch_rejects_bad_plans(pkg):
     exact.close()
     for s in solvers:
         s.close()
+
+
+def test_batch_matches_oracle_directly(pkg):
+    """Each solve of a batch against the oracle's own driver loop (not only
+    against solo GPU runs): three uneven channel grids, 400 adaptive steps in
+    launches of 150, every conserved plane within 1e-12 relative L-inf and the
+    same simulated time."""
+    from oracle import bind
+    cfgs = [cases.channel_config(L=48, M=20, a=0.1),
+            cases.channel_config(L=100, M=40, vz=0.2, beta=0.3),
+            cases.channel_config(L=64, M=30, amp=1.5, a=0.15)]
+    solvers = [pkg.build_case(c, precision="fast") for c in cfgs]
+    batch = pkg.BatchSolver(solvers)
+    res = batch.run(pkg.BatchPlan([2, 1], [0, 1, 0]), T=1e300, adaptive=True, max_steps=400,
+                    steps_per_launch=150)
+    for i, cfg in enumerate(cfgs):
+        assert res.runs[i].steps == 400
+        case = cases.make_case(cfg)
+        o = bind.Port(case.oracle_dict())
+        ran = o.run(1e300, cfg.dt, True, cfg.cfl_number, cfg.dt_growth_factor, cfg.dt_min,
+                    cfg.dt_max, max_steps=400)
+        assert ran["steps"] == 400
+        assert abs(res.runs[i].t - ran["t"]) <= 1e-12 * ran["t"], i
+        got, want = solvers[i].conserved(), o.conserved()
+        for k in range(8):
+            den = np.abs(want[k]).max()
+            assert np.abs(got[k] - want[k]).max() <= 1e-12 * (den if den > 0 else 1.0), (i, k)
+        o.close()
+    batch.close()
+    for s in solvers:
+        s.close()

@@ -241,6 +241,85 @@ def test_restart_set_physical_and_snapshot(pkg):
     other.close()
 
 
+def test_snapshot_mid_run_captures_its_step(pkg):
+    """IOManager's snapshot (src/io_manager.cpp:68-77) taken while stepping
+    goes on: mpd_snapshot_async at step 40 of the 200 x 80 channel (exact
+    precision), then 60 more steps through the graph run loop on the solver's
+    stream while the copies run on the side stream; the pinned buffer must
+    hold the oracle's physical planes of step 40 bit for bit, and the state
+    after step 100 must equal the oracle's too (the snapshot did not disturb
+    the stepping)."""
+    import torch
+    case = cases.channel_case(L=200, M=80, a=0.1)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="exact")
+    oracle = bind.Port(case.oracle_dict())
+    dt = step_both(solver, oracle, cfg, 40, cfg.dt)
+    at40 = oracle.physical()
+    buf = torch.empty((10,) + solver.shape, dtype=torch.float64).pin_memory()
+    solver.snapshot_async(buf)
+    res = solver.run(T=1e300, dt=dt, adaptive=True, max_steps=60)
+    solver.snapshot_wait()
+    np.testing.assert_array_equal(buf.numpy(), at40)
+    assert res.steps == 60
+    cases.run_oracle_steps(oracle, 60, dt, cfg)
+    np.testing.assert_array_equal(solver.conserved(), oracle.conserved())
+    solver.close()
+    oracle.close()
+
+
+def test_run_monitor_reports_match_oracle(pkg):
+    """The driver loop's periodic reports from inside mpd_run
+    (src/main.cpp:249-281): on the 200 x 80 channel (exact precision, adaptive
+    dt) a 2500-step run reports at steps 1000 and 2000 the checkpoint cell's
+    values, t, the next dt and the wave speed bit for bit as the oracle, the
+    conserved integrals within 1e-13, and no CheckCfl warning; the run itself
+    ends in the oracle's state."""
+    case = cases.channel_case(L=200, M=80, a=0.1)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="exact")
+    reps = []
+    res = solver.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=2500, monitor=reps.append,
+                     monitor_every=1000)
+    assert res.steps == 2500
+    assert [r.step for r in reps] == [1000, 2000]
+    oracle = bind.Port(case.oracle_dict())
+    dt, t = cfg.dt, 0.0
+    for rep in reps:
+        for _ in range(1000):
+            oracle.advance(dt)
+            t += dt
+            dt = oracle.compute_dt(cfg.cfl_number, cfg.dt_growth_factor, cfg.dt_min, cfg.dt_max,
+                                   dt)
+        phys = oracle.physical()
+        assert list(rep.probe) == [phys[k][21, 41] for k in (0, 1, 3, 4, 9)]
+        assert (rep.t, rep.dt) == (t, dt)
+        assert rep.max_wave_speed == oracle.max_wave_speed()
+        assert not rep.cfl_warning
+        np.testing.assert_allclose(rep.integrals, oracle.integrals(), rtol=1e-13, atol=0)
+    cases.run_oracle_steps(oracle, 500, dt, cfg)
+    np.testing.assert_array_equal(solver.conserved(), oracle.conserved())
+    solver.close()
+    oracle.close()
+
+
+def test_run_monitor_flags_cfl_warning(pkg):
+    """A fixed dt above the CFL limit: every report carries CheckCfl's warning
+    (src/diagnostics.cpp:112-125), with the wave speed of the state."""
+    case = cases.channel_case(L=200, M=80)
+    cfg = case.cfg
+    solver = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+    reps = []
+    solver.run(T=1e300, dt=1.7e-3, adaptive=False, max_steps=1000, monitor=reps.append,
+               monitor_every=500)
+    assert [r.step for r in reps] == [500, 1000]
+    for r in reps:
+        assert r.cfl_warning and r.dt == 1.7e-3 and r.dt_cfl < 1.7e-3
+        assert r.dt_cfl == cfg.cfl_number * min(cfg.dz, cfg.dy) / (r.max_wave_speed + 1e-10)
+    assert reps[-1].max_wave_speed == solver.MaxWaveSpeed()
+    solver.close()
+
+
 def test_full_size_channel_fast_vs_oracle(pkg):
     """The 1600 x 640 channel (440 blocks of TMA strips and bands): the fast
     path through the graph run loop against the oracle's own driver loop
