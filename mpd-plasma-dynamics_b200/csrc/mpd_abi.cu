@@ -15,6 +15,7 @@
 #include "bc_compile.hpp"
 #include "kernels.cuh"
 #include "lf_fast.cuh"
+#include "lf_pair.cuh"
 #include "lf_persist.cuh"
 #include "lf_tma.cuh"
 
@@ -71,13 +72,14 @@ EncodeTiledFn GetEncodeTiled() {
 
 // The 8 conserved planes of one state buffer as a 3-D tensor
 // {columns M+3, rows L+2, planes 8} with the row pitch and plane stride of the
-// allocation; tiles are {32 columns, 1 row, 8 planes}, zero-filled outside.
-int EncodeStateMap(CUtensorMap *map, double *base, int cols, int rows, int pitch, size_t ps) {
+// allocation; tiles are {box_cols columns, 1 row, 8 planes}, zero-filled outside.
+int EncodeStateMap(CUtensorMap *map, double *base, int cols, int rows, int pitch, size_t ps,
+                   int box_cols) {
     EncodeTiledFn enc = GetEncodeTiled();
     if (!enc) return Fail(MPD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable from the driver");
     const cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, 8};
     const cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(double), (cuuint64_t)ps * sizeof(double)};
-    const cuuint32_t box[3] = {32, 1, 8};
+    const cuuint32_t box[3] = {(cuuint32_t)box_cols, 1, 8};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -104,7 +106,9 @@ struct mpd_solver {
     int len = 0;                             // line length
     int resid_blocks = 0;                    // residual_kernel: one resident wave
     CUtensorMap tmap[2];                     // conserved planes of buf[0] / buf[1]
+    CUtensorMap tmap_pair[2];                // the same with 64-column tiles
     mpd::TmaPlan plan;                       // one-wave strips x bands
+    mpd::TmaPlan pair_plan;                  // the same for lf_pair_kernel
     mpd::TmaPlan pplan;                      // persistent launch (cooperative wave)
     bool persist_ok = false;                 // the persistent engine can run here
     mpd::GridSync *gsync = nullptr;          // its barrier and reduction words
@@ -261,7 +265,15 @@ int InitFromIc(mpd_solver *s) {
 // the guarded relative-L2 convergence check and, every residual_every steps,
 // the L-inf residual.  want_ws: fuse the maximum
 // wave speed (adaptive dt and the per-call ComputeDt need it).
-int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool want_ws) {
+// Interior kernel of fast steps >= 1 on the graph and per-call paths:
+// lf_pair_kernel (two point columns per lane) unless MPD_INTERIOR_PAIR is 0;
+// both give the same bits, the persistent engines use the one-column form.
+#ifndef MPD_INTERIOR_PAIR
+#define MPD_INTERIOR_PAIR 1
+#endif
+
+int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool want_ws,
+                   int variant = MPD_INTERIOR_PAIR) {
     const mpd::Geo &g = s->g;
     const int usd = use_state_dt ? 1 : 0;
     if (first || s->precision == MPD_PRECISION_EXACT) {
@@ -273,6 +285,10 @@ int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool
         else
             mpd::lf_exact_kernel<false><<<grid, block, 0, s->stream>>>(
                 g, s->buf[0], s->buf[1], s->ic, s->st, dt, usd, s->cphys, s->len);
+    } else if (variant) {
+        MPD_CK(mpd::launch_lf_pair(g, s->pair_plan, s->tmap_pair[0], s->tmap_pair[1], s->buf[0],
+                                   s->buf[1], s->st, dt, usd, want_ws, s->cphys, s->len,
+                                   s->stream));
     } else {
         MPD_CK(mpd::launch_lf_tma(g, s->plan, s->tmap[0], s->tmap[1], s->buf[0], s->buf[1],
                                   s->st, dt, usd, want_ws, s->cphys, s->len, s->stream));
@@ -508,8 +524,12 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
     }
     if (s->precision == MPD_PRECISION_FAST) {
         for (int b = 0; b < 2; ++b)
-            STEP(EncodeStateMap(&s->tmap[b], s->buf[b], s->cols, s->rows, s->pitch, s->ps));
-        if (mpd::plan_lf_tma(g, s->device, s->plan) != cudaSuccess) {
+            STEP(EncodeStateMap(&s->tmap[b], s->buf[b], s->cols, s->rows, s->pitch, s->ps, 32));
+        for (int b = 0; b < 2; ++b)
+            STEP(EncodeStateMap(&s->tmap_pair[b], s->buf[b], s->cols, s->rows, s->pitch, s->ps,
+                                64));
+        if (mpd::plan_lf_tma(g, s->device, s->plan) != cudaSuccess ||
+            mpd::plan_lf_pair(g, s->device, s->pair_plan) != cudaSuccess) {
             FreeAll(s);
             return Fail(MPD_ERR_CUDA, "occupancy query for the interior kernel failed");
         }
@@ -1232,7 +1252,9 @@ int mpd_profile_kernels(mpd_solver *s, int steps, double dt, double out_ms[2]) {
 int mpd_profile_kernel(mpd_solver *s, int which, int launches, double dt, double *ms) {
     int rc = CheckHandle(s);
     if (rc != MPD_OK) return rc;
-    if (launches <= 0 || !ms || (which != MPD_KERNEL_INTERIOR && which != MPD_KERNEL_RESIDUAL))
+    if (launches <= 0 || !ms ||
+        (which != MPD_KERNEL_INTERIOR && which != MPD_KERNEL_RESIDUAL &&
+         which != MPD_KERNEL_INTERIOR_1COL))
         return Fail(MPD_ERR_INVALID, "bad profile request");
     rc = SyncState(s);
     if (rc != MPD_OK) return rc;
@@ -1242,6 +1264,8 @@ int mpd_profile_kernel(mpd_solver *s, int which, int launches, double dt, double
     for (int i = 0; i < launches && rc == MPD_OK; ++i) {
         if (which == MPD_KERNEL_INTERIOR) {
             rc = LaunchInterior(s, false, false, dt, true);
+        } else if (which == MPD_KERNEL_INTERIOR_1COL) {
+            rc = LaunchInterior(s, false, false, dt, true, 0);
         } else {
             mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0],
                                                                          s->buf[1], s->st, 1);
@@ -1256,7 +1280,7 @@ int mpd_profile_kernel(mpd_solver *s, int which, int launches, double dt, double
     *ms = static_cast<double>(t) / launches;
     // the interior launches folded this dt's wave speed into the step's
     // accumulator: clear it, so the next step's controller sees only its own
-    if (which == MPD_KERNEL_INTERIOR) {
+    if (which != MPD_KERNEL_RESIDUAL) {
         MPD_CK(cudaMemsetAsync(&s->st->ws_acc, 0, sizeof(unsigned long long), s->stream));
         MPD_CK(cudaMemsetAsync(&s->st->nf_acc, 0, sizeof(unsigned int), s->stream));
         MPD_CK(cudaStreamSynchronize(s->stream));
