@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--diagnostics", action="store_true",
                     help="with --profile: then each reduction once (residual, integrals, "
                          "solution change, outlet, radial symmetry, wave speed)")
+    ap.add_argument("--one-column", action="store_true",
+                    help="with --profile: then three launches of the one-column interior "
+                         "kernel (the persistent engines' form) on the final state")
     ap.add_argument("--precision", choices=("fast", "exact"), default="fast")
     ap.add_argument("--workload", choices=("plain", "warmstart", "batch", "surrogate", "serve",
                                            "converge"),
@@ -611,6 +614,8 @@ def run_profile(args):
         solver.Advance(dt)
     t, step = solver.time()
     out = {"profile_steps": args.steps, "step": step, "t": t}
+    if args.one_column:
+        out["one_column_ms"] = solver.profile_kernel("interior_1col", 3, dt)
     if args.diagnostics:
         out["residual"] = solver.residual()
         out["integrals"] = [float(x) for x in solver.ComputeIntegrals()]
