@@ -72,6 +72,19 @@ def parse():
                          "without it serve trains a small one first")
     ap.add_argument("--save", type=str, default="", help="warmstart: save the surrogate here")
     ap.add_argument("--big", type=str, default="4096x1600")
+    ap.add_argument("--bootstrap", type=str, default="",
+                    help="warmstart: generate the training data warm from a surrogate first "
+                         "trained on this coarser grid (e.g. 100x40)")
+    ap.add_argument("--n-boot", type=int, default=2000)
+    ap.add_argument("--plain-sample", type=int, default=32,
+                    help="warmstart: solves of the plain march timed one after another")
+    ap.add_argument("--warm-fraction", type=float, default=1.0,
+                    help="warmstart: a warm solve's step budget as a fraction of the cold "
+                         "estimate before it falls back to the cold start")
+    ap.add_argument("--tight-tol", type=float, default=1e-10)
+    ap.add_argument("--stage", choices=("all", "build", "eval"), default="all",
+                    help="warmstart: build = data + training (--save), eval = the held-out "
+                         "comparison with a saved surrogate (--surrogate), all = both")
     return ap.parse_args()
 
 
@@ -401,18 +414,34 @@ def run_ours(args, rank, world, local_rank):
 
 def run_warmstart(args):
     """Learned warm start (the sweep box on one grid): steady states from the
-    batched solver train the surrogate; held-out draws are then solved cold
-    and warm by the batched solver, and a sample of them one after another by
-    the plain FP64 time march (graph engine).  value = warm-start batch
-    solves/s (surrogate inference included)."""
+    batched solver train the surrogate (on a fine grid, optionally
+    bootstrapped from a coarse surrogate's interpolated predictions);
+    held-out draws are then solved cold and warm by the batched solver (warm
+    solves judged and backed by the plain march), and a sample of them one
+    after another by the plain FP64 time march (graph engine).  value =
+    warm-start batch solves/s (surrogate inference included)."""
     import __graft_entry__
     pkg = __graft_entry__.load_package()
+    WS = pkg.warmstart
     L, M = (int(v) for v in args.grid.split("x"))
-    res = pkg.warmstart.run_pipeline(n_train=args.n_train, n_eval=args.n_eval, grid=(L, M),
-                                     epochs=args.epochs, max_steps=args.max_steps,
-                                     log=lambda m: print(m, file=sys.stderr, flush=True),
-                                     save=args.save or None)
-    losses = res.pop("losses")
+    boot = tuple(int(v) for v in args.bootstrap.split("x")) if args.bootstrap else None
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    info = {}
+    if args.stage == "eval":
+        tr = WS.Trained.load(args.surrogate)
+    else:
+        tr, info = WS.build_surrogate(args.n_train, (L, M), args.epochs, max_steps=args.max_steps,
+                                      bootstrap=boot, n_boot=args.n_boot, log=log,
+                                      save=args.save or None)
+        info.pop("losses", None)
+        if args.stage == "build":
+            return {"metric": "learned warm start: surrogate built", "value": info["train_s"],
+                    "unit": "s", "higher_is_better": False, "n_gpus": 1,
+                    "data": "synthetic (sweep-box draws, numpy default_rng(seed))",
+                    "config": {"workload": f"learned warm start, training on {L}x{M}",
+                               "bootstrap": args.bootstrap or None}, **info}
+    res = WS.evaluate(tr, args.n_eval, (L, M), args.max_steps, plain_sample=args.plain_sample,
+                      warm_fraction=args.warm_fraction, tight_tol=args.tight_tol, log=log)
     return {
         "metric": "steady solves/s, warm-start batch (residual <= 1e-8)",
         "value": res["warm_batch_solves_per_s"], "unit": "solves/s", "n_gpus": 1,
@@ -420,8 +449,9 @@ def run_warmstart(args):
         "data": "synthetic (sweep-box draws, numpy default_rng(seed))",
         "config": {"workload": f"learned warm start, channel sweep box on {L}x{M}",
                    "n_train": args.n_train, "n_eval": args.n_eval, "epochs": args.epochs,
+                   "bootstrap": args.bootstrap or None,
                    "surrogate": "4 spectral layers, 64 channels, 8 modes per axis"},
-        "vs_baseline": None, "loss_first_last": [losses[0], losses[-1]], **res}
+        "vs_baseline": None, **info, **res}
 
 
 def run_converge(args):

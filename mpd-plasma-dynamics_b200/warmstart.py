@@ -12,9 +12,16 @@ Pipeline:
      of the workload (cold) and from the surrogate's prediction (warm);
      steps to converge, solves per second and the surrogate's own L-inf error
      against the converged state are reported.  The plain time march stays
-     the judge: a warm solve is accepted only at residual <= tol, and a
-     prediction that fails (non-finite, non-positive density or energy) falls
-     back to the cold initial condition.
+     the judge and the fallback: a warm solve is accepted only at residual
+     <= tol within its step budget; a non-finite prediction, or a warm solve
+     that ends non-finite or unconverged within the budget, is solved again
+     from the cold initial condition (solve_warm).
+
+On a fine grid the training data itself is generated warm (bootstrap): a
+surrogate trained on a coarse grid predicts each fine training draw, the
+prediction is interpolated bilinearly onto the fine grid, and the plain march
+converges from it (with the same fallback).  run_pipeline does all of it in
+one call; build_surrogate and evaluate split it in two.
 """
 from __future__ import annotations
 
@@ -25,7 +32,7 @@ import time
 import numpy as np
 
 from . import surrogate as S
-from .batch import Autotuner, BatchPlan, BatchSolver
+from .batch import Autotuner, BatchPlan, BatchSolver, estimated_steps
 from .geometry import GeometryRegistry, Grid
 from .ic import ArrayIC, derived_pressures
 from .solver import GpuSolver, build_case
@@ -121,17 +128,103 @@ def solve_all(params: list[SweepParams], ics: list | None = None, max_steps=200_
     return SolveSet(steps, conv, res, fields, dev_ms, solve_ms)
 
 
+def upsample_fields(f: np.ndarray, L: int, M: int) -> np.ndarray:
+    """Bilinear interpolation of H x W x 8 point fields of a coarse grid
+    (points at z = i / H, y = j / (W - 1)) onto the points of an L x M grid
+    (z = i / L, y = j / M); rows past the coarse grid's last take its values."""
+    Hc, Wc = f.shape[:2]
+    zi = np.minimum(np.arange(L) * (Hc / L), Hc - 1)
+    yj = np.arange(M + 1) * ((Wc - 1) / M)
+    i0 = np.minimum(np.floor(zi).astype(int), Hc - 2) if Hc > 1 else np.zeros(L, int)
+    j0 = np.minimum(np.floor(yj).astype(int), Wc - 2)
+    wi = (zi - i0)[:, None, None]
+    wj = (yj - j0)[None, :, None]
+    i1 = np.minimum(i0 + 1, Hc - 1)
+    a = f[i0][:, j0] * (1 - wj) + f[i0][:, j0 + 1] * wj
+    b = f[i1][:, j0] * (1 - wj) + f[i1][:, j0 + 1] * wj
+    return a * (1 - wi) + b * wi
+
+
+def _empty_set(n: int) -> SolveSet:
+    return SolveSet(np.zeros(n, dtype=np.int64), np.zeros(n, dtype=bool), np.full(n, np.nan),
+                    [None] * n, 0.0, np.zeros(n))
+
+
+def solve_warm(params: list[SweepParams], ics: list, max_steps=200_000, tol=1e-8, every=50,
+               budget: int | None = None, chunk: int = 256) -> tuple[SolveSet, np.ndarray]:
+    """Warm solves judged by the plain march: solve i starts from ics[i]
+    (10 physical planes) at its CFL dt and has `budget` steps (default: half
+    the cold estimate, estimated_steps) to reach the L-inf residual tol.  A
+    missing (None: non-finite) prediction, and a warm solve that ends
+    non-finite or unconverged within the budget, is solved again from the
+    workload's initial condition with max_steps.  Returns the combined set
+    (steps, device and per-solve times of both attempts added) and the mask of
+    solves that fell back."""
+    n = len(params)
+    out = _empty_set(n)
+    fell = np.array([ic is None for ic in ics])
+    use = np.flatnonzero(~fell)
+    if budget is None:
+        budget = max(1000, estimated_steps(params[0].config(), max_steps) // 2)
+    if len(use):
+        w = solve_all([params[i] for i in use], ics=[ics[i] for i in use],
+                      max_steps=min(budget, max_steps), tol=tol, every=every, chunk=chunk)
+        out.device_ms += w.device_ms
+        for k, i in enumerate(use):
+            out.steps[i], out.converged[i], out.residual[i] = w.steps[k], w.converged[k], \
+                w.residual[k]
+            out.fields[i], out.solve_ms[i] = w.fields[k], w.solve_ms[k]
+            if not w.converged[k]:
+                fell[i] = True
+    back = np.flatnonzero(fell)
+    if len(back):
+        c = solve_all([params[i] for i in back], max_steps=max_steps, tol=tol, every=every,
+                      chunk=chunk)
+        out.device_ms += c.device_ms
+        for k, i in enumerate(back):
+            out.steps[i] += c.steps[k]
+            out.converged[i], out.residual[i] = c.converged[k], c.residual[k]
+            out.fields[i] = c.fields[k]
+            out.solve_ms[i] += c.solve_ms[k]
+    return out, fell
+
+
+def predicted_ics(tr: "Trained", params: list[SweepParams], grid, floor) -> tuple[list, float]:
+    """Initial planes predicted by the surrogate for each draw on `grid`
+    (None where the prediction is not finite) and the inference seconds.  A
+    surrogate trained on another (coarser) grid predicts on its own grid and
+    the prediction is interpolated bilinearly."""
+    L, M = grid
+    Hs, Ws = tr.net.H, tr.net.W
+    src_grid = (Hs, Ws - 1)
+    g = grid_of(draws([0], src_grid)[0].config())
+    X = np.stack([inputs_of(p, g) for p in params])
+    pred, infer_s = predict(tr, X)
+    out = []
+    for p, f in zip(params, pred):
+        f = f.reshape(Hs, Ws, S.N_OUT)
+        if not np.all(np.isfinite(f)):
+            out.append(None)
+            continue
+        if (Hs, Ws) != (L, M + 1):
+            f = upsample_fields(f, L, M)
+        out.append(planes_from_fields(f, p.config(), floor))
+    return out, infer_s
+
+
 @dataclasses.dataclass
 class Trained:
     net: S.SpectralOperator
     norm: S.Normalizer
     losses: list
     train_s: float
+    floor: np.ndarray | None = None   # lower bounds of predicted rho and e
 
     def save(self, path):
         p = self.net.get_params()
+        floor = self.floor if self.floor is not None else np.zeros(2)
         np.savez(path, H=self.net.H, W=self.net.W, mean=self.norm.mean, std=self.norm.std,
-                 const=self.norm.const, losses=np.array(self.losses),
+                 const=self.norm.const, losses=np.array(self.losses), floor=floor,
                  **{f"p_{k}": v for k, v in p.items()})
 
     @classmethod
@@ -140,7 +233,8 @@ class Trained:
         params = {k[2:]: z[k] for k in z.files if k.startswith("p_")}
         net = S.SpectralOperator(int(z["H"]), int(z["W"]), batch, params=params)
         norm = S.Normalizer(z["mean"], z["std"], z["const"])
-        return cls(net, norm, list(z["losses"]), 0.0)
+        floor = z["floor"] if "floor" in z.files else None
+        return cls(net, norm, list(z["losses"]), 0.0, floor)
 
 
 def train(X: np.ndarray, Y: np.ndarray, H: int, W: int, epochs: int = 40, batch: int = 16,
@@ -227,54 +321,71 @@ def tight_agreement(params, cold: SolveSet, warm: SolveSet, idx, tol: float,
     return dist, w.steps
 
 
-def run_pipeline(n_train=2000, n_eval=256, grid=(100, 40), epochs=40, batch=16, lr=1e-3,
-                 max_steps=200_000, tol=1e-8, plain_sample=4, log=print,
-                 save: str | None = None, tight_tol: float = 1e-10,
-                 tight_sample: int = 16) -> dict:
-    """Steps 1-3 of the module docstring; returns the measurements.  A sample
-    of `tight_sample` solves converged both ways is then driven on to
-    `tight_tol` to show the warm and cold steady states agree once both are
-    converged that far."""
+def build_surrogate(n_train=2000, grid=(100, 40), epochs=40, batch=16, lr=1e-3,
+                    max_steps=200_000, tol=1e-8, bootstrap=None, n_boot=2000, boot_epochs=60,
+                    boot_max_steps=200_000, log=print, save: str | None = None,
+                    ) -> tuple[Trained, dict]:
+    """Steps 1-2 of the module docstring: training steady states for the
+    draws 0 .. n_train-1 of the sweep box on `grid`, and the network trained
+    on them.  With bootstrap = a coarser (L, M), the training solves start
+    from the prediction of a surrogate first built the same way on that grid
+    (n_boot draws), interpolated onto `grid`."""
     L, M = grid
     H, W = L, M + 1
     train_p = draws(range(n_train), grid)
-    eval_p = draws(range(1_000_000, 1_000_000 + n_eval), grid)
-    tuner = None
+    info: dict = {"grid": f"{L}x{M}", "n_train": n_train, "epochs": epochs}
     t0 = time.perf_counter()
-    data = solve_all(train_p, max_steps=max_steps, tol=tol)
+    if bootstrap and tuple(bootstrap) != tuple(grid):
+        coarse, cinfo = build_surrogate(n_boot, tuple(bootstrap), boot_epochs, batch, lr,
+                                        max_steps=boot_max_steps, tol=tol, log=log)
+        info["bootstrap"] = cinfo
+        ics, _ = predicted_ics(coarse, train_p, grid, coarse.floor)
+        del coarse  # its device buffers go back to the allocator
+        data, fell = solve_warm(train_p, ics, max_steps=max_steps, tol=tol, budget=max_steps)
+        info["bootstrap_fallbacks"] = int(fell.sum())
+    else:
+        data = solve_all(train_p, max_steps=max_steps, tol=tol)
     gen_s = time.perf_counter() - t0
     keep = np.flatnonzero(data.converged)
-    log(f"training solves: {len(keep)} of {n_train} converged, {gen_s:.1f} s")
-    grids = [grid_of(p.config()) for p in train_p[:1]]
-    X = np.stack([inputs_of(train_p[i], grids[0]) for i in keep])
+    log(f"training solves on {L}x{M}: {len(keep)} of {n_train} converged, {gen_s:.1f} s")
+    g0 = grid_of(train_p[0].config())
+    X = np.stack([inputs_of(train_p[i], g0) for i in keep])
     Y = np.stack([data.fields[i].reshape(H * W, S.N_OUT) for i in keep])
     tr = train(X, Y, H, W, epochs=epochs, batch=batch, lr=lr, log=log)
+    tr.floor = np.array([0.05 * np.min(Y[..., 0]), 0.05 * np.min(Y[..., 4])])
     log(f"trained {epochs} epochs in {tr.train_s:.1f} s, final loss {tr.losses[-1]:.3e}")
     if save:
         tr.save(save)
+    info.update({"n_train_converged": int(len(keep)), "data_gen_s": gen_s,
+                 "data_steps_median": float(np.median(data.steps)),
+                 "data_device_s": data.device_ms * 1e-3, "train_s": tr.train_s,
+                 "final_loss": tr.losses[-1], "losses": tr.losses})
+    return tr, info
 
-    Xe = np.stack([inputs_of(p, grids[0]) for p in eval_p])
-    pred, infer_s = predict(tr, Xe)
-    floor = np.array([0.05 * np.min(Y[..., 0]), 0.05 * np.min(Y[..., 4])])
-    cfg0 = eval_p[0].config()
-    ics = []
-    fallback = 0
-    for p, f in zip(eval_p, pred):
-        f = f.reshape(H, W, S.N_OUT)
-        if not np.all(np.isfinite(f)):
-            ics.append(None)
-            fallback += 1
-            continue
-        ics.append(planes_from_fields(f, p.config(), floor))
+
+def evaluate(tr: Trained, n_eval=256, grid=(100, 40), max_steps=200_000, tol=1e-8,
+             plain_sample=32, warm_fraction=1.0, tight_tol: float = 1e-10,
+             tight_sample: int = 16, log=print) -> dict:
+    """Step 3 of the module docstring on the held-out draws 1e6 .. 1e6 +
+    n_eval - 1: cold and warm batches (the warm one judged and backed by the
+    plain march, solve_warm, with warm_fraction of the cold step estimate as
+    its budget), the plain FP64 march one solve after another on
+    `plain_sample` of them, and `tight_sample` solves converged both ways
+    driven on to tight_tol."""
+    L, M = grid
+    H, W = L, M + 1
+    eval_p = draws(range(1_000_000, 1_000_000 + n_eval), grid)
+    floor = tr.floor if tr.floor is not None else np.zeros(2)
+    ics, infer_s = predicted_ics(tr, eval_p, grid, floor)
     cold = solve_all(eval_p, max_steps=max_steps, tol=tol)
-    warm = solve_all(eval_p, ics=ics, max_steps=max_steps, tol=tol)
+    budget = max(1000, int(warm_fraction * estimated_steps(eval_p[0].config(), max_steps)))
+    warm, fell = solve_warm(eval_p, ics, max_steps=max_steps, tol=tol, budget=budget)
     both = cold.converged & warm.converged
-    log(f"eval: cold converged {int(cold.converged.sum())}, warm converged "
-        f"{int(warm.converged.sum())} of {n_eval}; steps cold median "
-        f"{np.median(cold.steps):.0f}, warm median {np.median(warm.steps):.0f}; warm residuals "
-        f"{np.nanmedian(warm.residual):.2e}")
-    err = [relative_linf(pred[i].reshape(H, W, S.N_OUT), cold.fields[i])
-           for i in np.flatnonzero(cold.converged)]
+    log(f"eval on {L}x{M}: cold converged {int(cold.converged.sum())}, warm converged "
+        f"{int(warm.converged.sum())} of {n_eval} ({int(fell.sum())} fell back); steps cold "
+        f"median {np.median(cold.steps):.0f}, warm median {np.median(warm.steps):.0f}")
+    err = [relative_linf(fields_of(ics[i], L, M), cold.fields[i])
+           for i in np.flatnonzero(cold.converged) if ics[i] is not None]
     err = np.stack(err) if err else np.full((1, S.N_OUT), np.nan)
     agree = [relative_linf(warm.fields[i], cold.fields[i]) for i in np.flatnonzero(both)]
     agree = np.stack(agree) if agree else None
@@ -282,7 +393,7 @@ def run_pipeline(n_train=2000, n_eval=256, grid=(100, 40), epochs=40, batch=16, 
     tight_idx = np.flatnonzero(both)[:tight_sample]
     tight = None
     if len(tight_idx) and tight_tol and tight_tol < tol:
-        dist, extra = tight_agreement(eval_p, cold, warm, tight_idx, tight_tol, max_steps)
+        dist, extra = tight_agreement(eval_p, cold, warm, tight_idx, tight_tol, 4 * max_steps)
         tight = {"tol": tight_tol, "sample": int(len(tight_idx)),
                  "warm_vs_cold_rel_linf_max": dist.tolist(),
                  "extra_steps_median": float(np.median(extra))}
@@ -290,29 +401,30 @@ def run_pipeline(n_train=2000, n_eval=256, grid=(100, 40), epochs=40, batch=16, 
             f"{np.nanmax(dist):.2e} over {len(tight_idx)} solves")
 
     # the plain FP64 time march, one solve after another (graph engine)
-    seq_ms, seq_steps = 0.0, 0
+    seq_ms, seq_steps, seq_conv = 0.0, 0, 0
     for p in eval_p[:plain_sample]:
-        s = build_case(p.config(), precision="fast")
-        r = s.run(T=1e300, dt=cfg0.dt, adaptive=True, max_steps=max_steps, residual_tol=tol,
+        cfg = p.config()
+        s = build_case(cfg, precision="fast")
+        r = s.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=max_steps, residual_tol=tol,
                   residual_every=50, engine="graph")
         seq_ms += r.device_ms
         seq_steps += r.steps
+        seq_conv += int(r.converged)
         s.close()
-    plain_sps = plain_sample / (seq_ms * 1e-3)
+    plain_sps = plain_sample / (seq_ms * 1e-3) if plain_sample else float("nan")
     cold_sps = n_eval / (cold.device_ms * 1e-3)
     warm_sps = n_eval / (warm.device_ms * 1e-3 + infer_s)
     return {
-        "grid": f"{L}x{M}", "n_train": n_train, "n_train_converged": int(len(keep)),
-        "n_eval": n_eval, "epochs": epochs, "data_gen_s": gen_s, "train_s": tr.train_s,
-        "final_loss": tr.losses[-1], "losses": tr.losses,
+        "n_eval": n_eval, "eval_max_steps": max_steps, "tol": tol,
         "cold_converged": int(cold.converged.sum()), "warm_converged": int(warm.converged.sum()),
-        "warm_fallback_to_cold_ic": fallback,
+        "warm_fallback_to_cold_ic": int(fell.sum()), "warm_budget_steps": budget,
         "cold_steps_mean": float(cold.steps.mean()), "warm_steps_mean": float(warm.steps.mean()),
         "cold_steps_median": float(np.median(cold.steps)),
         "warm_steps_median": float(np.median(warm.steps)),
         "cold_batch_solves_per_s": cold_sps, "warm_batch_solves_per_s": warm_sps,
         "plain_sequential_solves_per_s": plain_sps,
-        "plain_sequential_sample": plain_sample,
+        "plain_sequential_sample": plain_sample, "plain_sequential_converged": seq_conv,
+        "plain_sequential_steps_mean": seq_steps / max(plain_sample, 1),
         "warm_over_plain": warm_sps / plain_sps, "warm_over_cold_batch": warm_sps / cold_sps,
         "surrogate_inference_s": infer_s,
         "surrogate_rel_linf_median": np.median(err, 0).tolist(),
@@ -327,3 +439,15 @@ def run_pipeline(n_train=2000, n_eval=256, grid=(100, 40), epochs=40, batch=16, 
         "cold_p99_ms": float(np.percentile(cold.solve_ms, 99)),
         "tight": tight,
     }
+
+
+def run_pipeline(n_train=2000, n_eval=256, grid=(100, 40), epochs=40, batch=16, lr=1e-3,
+                 max_steps=200_000, tol=1e-8, plain_sample=32, log=print,
+                 save: str | None = None, tight_tol: float = 1e-10, tight_sample: int = 16,
+                 bootstrap=None, n_boot=2000, boot_epochs=60, warm_fraction=1.0) -> dict:
+    """build_surrogate then evaluate on the same grid; returns the measurements."""
+    tr, info = build_surrogate(n_train, grid, epochs, batch, lr, max_steps, tol, bootstrap,
+                               n_boot, boot_epochs, log=log, save=save)
+    res = evaluate(tr, n_eval, grid, max_steps, tol, plain_sample, warm_fraction, tight_tol,
+                   tight_sample, log)
+    return {**info, **res}

@@ -76,3 +76,29 @@ def test_trained_warm_start_beats_cold_start():
     # both runs stop at residual 1e-8, which leaves each about 1e-5 from the
     # exact fixed point of the scheme; they agree to that level
     assert max(res["warm_vs_cold_state_rel_linf_max"]) < 1e-4
+
+
+def test_untrained_surrogate_falls_back_to_cold_start():
+    """A deliberately poor surrogate (an untrained network): the plain march
+    stays the judge.  Its predictions get a small step budget; every solve
+    that does not reach the residual within it is solved again from the
+    workload's initial condition and then ends exactly as the cold solve
+    (same bits, same convergence), with both attempts' steps counted."""
+    WS, S = pkg.warmstart, pkg.surrogate
+    grid = (40, 16)
+    params = WS.draws(range(1_000_000, 1_000_006), grid)
+    cold = WS.solve_all(params, max_steps=200_000, tol=1e-8)
+    assert cold.converged.all()
+    Y = np.stack([f.reshape(-1, S.N_OUT) for f in cold.fields])
+    net = S.SpectralOperator(grid[0], grid[1] + 1, 16, seed=3)   # never trained
+    floor = np.array([0.05 * Y[..., 0].min(), 0.05 * Y[..., 4].min()])
+    tr = WS.Trained(net, S.Normalizer.fit(Y), [], 0.0, floor)
+    ics, _ = WS.predicted_ics(tr, params, grid, floor)
+    budget = int(0.1 * np.median(cold.steps))
+    warm, fell = WS.solve_warm(params, ics, max_steps=200_000, tol=1e-8, budget=budget)
+    assert fell.sum() >= len(params) // 2, fell
+    for i in np.flatnonzero(fell):
+        assert warm.converged[i] and warm.steps[i] >= cold.steps[i]
+        np.testing.assert_array_equal(warm.fields[i], cold.fields[i])
+    for i in np.flatnonzero(~fell):
+        assert warm.converged[i] and warm.steps[i] <= budget
