@@ -48,9 +48,9 @@ def parse():
     ap.add_argument("--diagnostics", action="store_true",
                     help="with --profile: then each reduction once (residual, integrals, "
                          "solution change, outlet, radial symmetry, wave speed)")
-    ap.add_argument("--one-column", action="store_true",
-                    help="with --profile: then three launches of the one-column interior "
-                         "kernel (the persistent engines' form) on the final state")
+    ap.add_argument("--pair", action="store_true",
+                    help="with --profile: then three launches of the two-column interior "
+                         "kernel (lf_pair_kernel) on the final state")
     ap.add_argument("--precision", choices=("fast", "exact"), default="fast")
     ap.add_argument("--workload", choices=("plain", "warmstart", "batch", "surrogate", "serve",
                                            "converge"),
@@ -249,9 +249,9 @@ def profiled_traffic(kernel: str = "lf_tma_kernel"):
 
 # ---------------------------------------------------------------- GPU side
 RESID_BYTES_PER_CELL = 128  # 8 new + 8 old conserved values read per interior cell
-# the interior kernel of fast steps (two point columns per lane); the
-# persistent engines' one-column form is timed beside it
-INTERIOR_KERNEL = "lf_pair_kernel"
+# the interior kernel of fast steps (one point column per lane, as in the
+# persistent engines); the two-column form is timed beside it
+INTERIOR_KERNEL = "lf_tma_kernel"
 
 
 def graph_chunk(steps: int) -> int:
@@ -325,7 +325,7 @@ def run_ours(args, rank, world, local_rank):
     # back-to-back launches between two events on the solver's stream
     hbm, hbm_src = measured_hbm()
     int_ms = solver.profile_kernel("interior", 30, res.dt)
-    int1_ms = solver.profile_kernel("interior_1col", 30, res.dt)
+    int2_ms = solver.profile_kernel("interior_pair", 30, res.dt)
     resid_ms = solver.profile_kernel("residual", 30, res.dt)
     achieved = ALG_BYTES_PER_CELL * CELLS / (int_ms * 1e-3) / 1e9
     resid_gbs = RESID_BYTES_PER_CELL * CELLS / (resid_ms * 1e-3) / 1e9
@@ -340,6 +340,13 @@ def run_ours(args, rank, world, local_rank):
     h_in = torch.from_numpy(np.ascontiguousarray(case.phys)).pin_memory()
     h_out = torch.empty(shape, dtype=torch.float64).pin_memory()
     n_e2e = args.steps
+    # one untimed pass of the same calls (the first upload creates the
+    # solver's dense staging planes)
+    solver.set_physical(h_in.numpy())
+    solver.Advance(cfg.dt)
+    solver.ComputeDt(cfg.dt)
+    solver.snapshot_async(h_out)
+    solver.snapshot_wait()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -386,7 +393,7 @@ def run_ours(args, rank, world, local_rank):
                          "frac": achieved / hbm, "traffic": traffic,
                          "traffic_note": traffic_note,
                          "kernel": INTERIOR_KERNEL, "kernel_ms": int_ms,
-                         "one_column_kernel_ms": int1_ms,
+                         "pair_kernel_ms": int2_ms,
                          "alg_bytes_per_launch": ALG_BYTES_PER_CELL * CELLS,
                          "kernel_timing": "30 back-to-back launches between two CUDA events",
                          "peak_source": hbm_src},
@@ -644,8 +651,8 @@ def run_profile(args):
         solver.Advance(dt)
     t, step = solver.time()
     out = {"profile_steps": args.steps, "step": step, "t": t}
-    if args.one_column:
-        out["one_column_ms"] = solver.profile_kernel("interior_1col", 3, dt)
+    if args.pair:
+        out["pair_ms"] = solver.profile_kernel("interior_pair", 3, dt)
     if args.diagnostics:
         out["residual"] = solver.residual()
         out["integrals"] = [float(x) for x in solver.ComputeIntegrals()]

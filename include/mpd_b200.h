@@ -251,12 +251,12 @@ int mpd_profile_kernels(mpd_solver *s, int steps, double dt, double out_ms[2]);
  * step dt; every launch recomputes the next step's interior cells from the
  * current state (the step counter does not advance; the state stays valid).
  * MPD_KERNEL_RESIDUAL: the L-inf residual pass over the current and previous
- * state.  MPD_KERNEL_INTERIOR_1COL: the one-point-column-per-lane interior
- * kernel of the persistent engines (fast precision; the same bits as the
- * default).  Needs a handle that has taken at least one step. */
+ * state.  MPD_KERNEL_INTERIOR_PAIR: the interior kernel's two-point-column-
+ * per-lane form (fast precision; the same bits as the default).  Needs a
+ * handle that has taken at least one step. */
 #define MPD_KERNEL_INTERIOR 0
 #define MPD_KERNEL_RESIDUAL 1
-#define MPD_KERNEL_INTERIOR_1COL 2
+#define MPD_KERNEL_INTERIOR_PAIR 2
 int mpd_profile_kernel(mpd_solver *s, int which, int launches, double dt, double *ms);
 
 /* ---- conserved integrals without allocating ----------------------------------- */

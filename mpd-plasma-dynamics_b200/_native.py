@@ -34,7 +34,7 @@ FACE_L_LO, FACE_L_HI, FACE_M_LO, FACE_M_HI = 0, 1, 2, 3
 NEUMANN, DIRICHLET, EXPRESSION, AXIS_LF = 0, 1, 2, 3
 ENGINE_AUTO, ENGINE_GRAPH, ENGINE_PERSISTENT = 0, 1, 2
 PRECISION_EXACT, PRECISION_FAST = 0, 1
-KERNEL_INTERIOR, KERNEL_RESIDUAL, KERNEL_INTERIOR_1COL = 0, 1, 2
+KERNEL_INTERIOR, KERNEL_RESIDUAL, KERNEL_INTERIOR_PAIR = 0, 1, 2
 PHYS_FIELDS = ("rho", "v_z", "v_r", "v_phi", "e", "p", "P", "H_z", "H_r", "H_phi")
 
 DP = C.POINTER(C.c_double)

@@ -837,26 +837,44 @@ __global__ void __launch_bounds__(kOutletThreads) outlet_kernel(StateBufs sb, do
 
 // Materialise the 10 physical planes of the current state (pitched); ghost
 // cells are zero as in the reference's Fields arrays.
+// The 10 physical planes of the current state, dense: plane k at
+// out + k (L+2)(M+3), cell (l, m) at l (M+3) + m (the host's layout, so one
+// contiguous copy moves them all).
 __global__ void phys_planes_kernel(StateBufs sb, double *out) {
     const StateView sv = sb.view();
     const Geo &g = sv.g;
     const int cols = g.M + 3, rows = g.L + 2;
     const int total = rows * cols;
+    const size_t ps = (size_t)total;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const int l = i / cols, m = i % cols;
         Phys q = phys_zero();
         if (l >= 1 && l <= g.L && m >= 1 && m <= g.M + 1) q = sv.phys(l, m);
-        const size_t o = g.ix(l, m);
-        out[0 * g.ps + o] = q.rho;
-        out[1 * g.ps + o] = q.vz;
-        out[2 * g.ps + o] = q.vr;
-        out[3 * g.ps + o] = q.vphi;
-        out[4 * g.ps + o] = q.e;
-        out[5 * g.ps + o] = q.p;
-        out[6 * g.ps + o] = q.P;
-        out[7 * g.ps + o] = q.Hz;
-        out[8 * g.ps + o] = q.Hr;
-        out[9 * g.ps + o] = q.Hphi;
+        out[0 * ps + i] = q.rho;
+        out[1 * ps + i] = q.vz;
+        out[2 * ps + i] = q.vr;
+        out[3 * ps + i] = q.vphi;
+        out[4 * ps + i] = q.e;
+        out[5 * ps + i] = q.p;
+        out[6 * ps + i] = q.P;
+        out[7 * ps + i] = q.Hz;
+        out[8 * ps + i] = q.Hr;
+        out[9 * ps + i] = q.Hphi;
+    }
+}
+
+// Interior cells (l in 1..L, m in 1..M+1) of 10 dense host-layout planes into
+// the pitched initial planes (their ghost cells are left as they are).
+__global__ void scatter_phys_kernel(Geo g, const double *dense, double *ic) {
+    const int cols = g.M + 3;
+    const int W = g.M + 1;
+    const int total = g.L * W;
+    const size_t dps = (size_t)(g.L + 2) * cols;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int l = 1 + i / W, m = 1 + i % W;
+        const size_t src = (size_t)l * cols + m, dst = g.ix(l, m);
+#pragma unroll
+        for (int k = 0; k < 10; ++k) ic[(size_t)k * g.ps + dst] = dense[(size_t)k * dps + src];
     }
 }
 

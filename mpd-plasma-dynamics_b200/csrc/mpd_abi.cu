@@ -214,6 +214,15 @@ int InitFromIc(mpd_solver *s);
 int UploadPhysical(mpd_solver *s, const double *phys10) {
     const size_t n = static_cast<size_t>(s->rows) * s->cols;
     MPD_CK(cudaMemsetAsync(s->ic, 0, 10 * s->ps * sizeof(double), s->stream));
+    if (phys10 && s->stage) {
+        // one contiguous copy into the dense staging planes, then the
+        // interior cells into the pitched planes on the device
+        MPD_CK(cudaMemcpyAsync(s->stage, phys10, 10 * n * sizeof(double), cudaMemcpyHostToDevice,
+                               s->stream));
+        mpd::scatter_phys_kernel<<<4 * 148, 256, 0, s->stream>>>(s->g, s->stage, s->ic);
+        MPD_CK(cudaGetLastError());
+        return InitFromIc(s);
+    }
     for (int k = 0; phys10 && k < 10; ++k) {
         const double *src = phys10 + k * n + s->cols + 1;  // (l=1, m=1)
         double *dst = s->ic + k * s->ps + s->pitch + 1;
@@ -266,10 +275,12 @@ int InitFromIc(mpd_solver *s) {
 // the L-inf residual.  want_ws: fuse the maximum
 // wave speed (adaptive dt and the per-call ComputeDt need it).
 // Interior kernel of fast steps >= 1 on the graph and per-call paths:
-// lf_pair_kernel (two point columns per lane) unless MPD_INTERIOR_PAIR is 0;
-// both give the same bits, the persistent engines use the one-column form.
+// lf_tma_kernel (one point column per lane), or lf_pair_kernel (two) with
+// MPD_INTERIOR_PAIR 1; both give the same bits.  Measured on a B200 at
+// 1600 x 640 (30 back-to-back launches): 26.3 us one column, 28.4 us pair
+// (8 resident warps per SM at 244 registers against 12 at 160).
 #ifndef MPD_INTERIOR_PAIR
-#define MPD_INTERIOR_PAIR 1
+#define MPD_INTERIOR_PAIR 0
 #endif
 
 int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool want_ws,
@@ -591,6 +602,8 @@ static int FinishRun(mpd_solver *s, long long step0, mpd_run_stats *stats) {
     MPD_CK(cudaEventSynchronize(s->ev1));
     float ms = 0.f;
     MPD_CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    rc = SyncState(s);  // the loop read the controller through its own slots
+    if (rc != MPD_OK) return rc;
     // the residual of the final state, when the loop stopped between checks
     if (!h.resid_valid && h.step > 0) {
         mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0], s->buf[1], s->st, 0);
@@ -1053,7 +1066,7 @@ int mpd_time(mpd_solver *s, double *t, long long *step) {
 
 static int MaterialisePhysical(mpd_solver *s) {
     if (!s->stage) {
-        int rc = DevAlloc(s, &s->stage, 10 * s->ps);
+        int rc = DevAlloc(s, &s->stage, 10 * static_cast<size_t>(s->rows) * s->cols);
         if (rc != MPD_OK) return rc;
     }
     if (s->snap_pending) MPD_CK(cudaStreamWaitEvent(s->stream, s->snap_ev, 0));
@@ -1074,7 +1087,13 @@ int mpd_download(mpd_solver *s, int which, double *host_plane) {
     } else {
         rc = MaterialisePhysical(s);
         if (rc != MPD_OK) return rc;
-        src = s->stage + (which - 8) * s->ps;
+        src = s->stage + (which - 8) * static_cast<size_t>(s->rows) * s->cols;
+        // the staging planes are dense: one contiguous copy
+        MPD_CK(cudaMemcpyAsync(host_plane, src,
+                               static_cast<size_t>(s->rows) * s->cols * sizeof(double),
+                               cudaMemcpyDeviceToHost, s->stream));
+        MPD_CK(cudaStreamSynchronize(s->stream));
+        return MPD_OK;
     }
     MPD_CK(cudaMemcpy2DAsync(host_plane, s->cols * sizeof(double), src, s->pitch * sizeof(double),
                              s->cols * sizeof(double), s->rows, cudaMemcpyDeviceToHost, s->stream));
@@ -1119,10 +1138,8 @@ int mpd_snapshot_async(mpd_solver *s, double *pinned_phys10) {
     MPD_CK(cudaEventRecord(s->stage_ev, s->stream));
     MPD_CK(cudaStreamWaitEvent(s->side, s->stage_ev, 0));
     const size_t n = static_cast<size_t>(s->rows) * s->cols;
-    for (int k = 0; k < 10; ++k)
-        MPD_CK(cudaMemcpy2DAsync(pinned_phys10 + k * n, s->cols * sizeof(double),
-                                 s->stage + k * s->ps, s->pitch * sizeof(double),
-                                 s->cols * sizeof(double), s->rows, cudaMemcpyDeviceToHost, s->side));
+    MPD_CK(cudaMemcpyAsync(pinned_phys10, s->stage, 10 * n * sizeof(double),
+                           cudaMemcpyDeviceToHost, s->side));
     MPD_CK(cudaEventRecord(s->snap_ev, s->side));
     s->snap_pending = true;
     return MPD_OK;
@@ -1143,6 +1160,10 @@ int mpd_set_physical(mpd_solver *s, const double *phys10) {
     MPD_CK(cudaStreamSynchronize(s->stream));
     if (s->snap_pending) MPD_CK(cudaEventSynchronize(s->snap_ev));
     s->snap_pending = false;
+    if (!s->stage) {  // the dense staging planes of the contiguous upload
+        rc = DevAlloc(s, &s->stage, 10 * static_cast<size_t>(s->rows) * s->cols);
+        if (rc != MPD_OK) return rc;
+    }
     return UploadPhysical(s, phys10);
 }
 
@@ -1254,7 +1275,7 @@ int mpd_profile_kernel(mpd_solver *s, int which, int launches, double dt, double
     if (rc != MPD_OK) return rc;
     if (launches <= 0 || !ms ||
         (which != MPD_KERNEL_INTERIOR && which != MPD_KERNEL_RESIDUAL &&
-         which != MPD_KERNEL_INTERIOR_1COL))
+         which != MPD_KERNEL_INTERIOR_PAIR))
         return Fail(MPD_ERR_INVALID, "bad profile request");
     rc = SyncState(s);
     if (rc != MPD_OK) return rc;
@@ -1264,8 +1285,8 @@ int mpd_profile_kernel(mpd_solver *s, int which, int launches, double dt, double
     for (int i = 0; i < launches && rc == MPD_OK; ++i) {
         if (which == MPD_KERNEL_INTERIOR) {
             rc = LaunchInterior(s, false, false, dt, true);
-        } else if (which == MPD_KERNEL_INTERIOR_1COL) {
-            rc = LaunchInterior(s, false, false, dt, true, 0);
+        } else if (which == MPD_KERNEL_INTERIOR_PAIR) {
+            rc = LaunchInterior(s, false, false, dt, true, 1);
         } else {
             mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0],
                                                                          s->buf[1], s->st, 1);

@@ -296,11 +296,11 @@ class GpuSolver:
 
     def profile_kernel(self, which: str, launches: int, dt: float) -> float:
         """Mean device ms of one launch of the interior kernel ("interior"),
-        its one-column form ("interior_1col") or the residual pass
+        its two-column form ("interior_pair") or the residual pass
         ("residual"), from back-to-back launches."""
         out = np.zeros(1)
         k = {"interior": N.KERNEL_INTERIOR, "residual": N.KERNEL_RESIDUAL,
-             "interior_1col": N.KERNEL_INTERIOR_1COL}[which]
+             "interior_pair": N.KERNEL_INTERIOR_PAIR}[which]
         self._call("mpd_profile_kernel", k, int(launches), float(dt), _dp(out))
         return float(out[0])
 

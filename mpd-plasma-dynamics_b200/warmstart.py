@@ -42,8 +42,8 @@ from .workloads import SweepParams, sweep_params
 PLANE_OF_FIELD = (0, 1, 2, 3, 4, 7, 8, 9)
 
 
-def draws(seeds, grid):
-    return [sweep_params(int(s), grids=(grid,)) for s in seeds]
+def draws(seeds, grid, a_max: float = 0.2):
+    return [sweep_params(int(s), grids=(grid,), a_max=a_max) for s in seeds]
 
 
 def grid_of(cfg) -> Grid:
@@ -324,20 +324,21 @@ def tight_agreement(params, cold: SolveSet, warm: SolveSet, idx, tol: float,
 def build_surrogate(n_train=2000, grid=(100, 40), epochs=40, batch=16, lr=1e-3,
                     max_steps=200_000, tol=1e-8, bootstrap=None, n_boot=2000, boot_epochs=60,
                     boot_max_steps=200_000, log=print, save: str | None = None,
-                    ) -> tuple[Trained, dict]:
+                    a_max: float = 0.2) -> tuple[Trained, dict]:
     """Steps 1-2 of the module docstring: training steady states for the
     draws 0 .. n_train-1 of the sweep box on `grid`, and the network trained
     on them.  With bootstrap = a coarser (L, M), the training solves start
     from the prediction of a surrogate first built the same way on that grid
-    (n_boot draws), interpolated onto `grid`."""
+    (n_boot draws), interpolated onto `grid`.  a_max widens the draws' wall
+    amplitude range beyond the sweep box's 0.2."""
     L, M = grid
     H, W = L, M + 1
-    train_p = draws(range(n_train), grid)
-    info: dict = {"grid": f"{L}x{M}", "n_train": n_train, "epochs": epochs}
+    train_p = draws(range(n_train), grid, a_max)
+    info: dict = {"grid": f"{L}x{M}", "n_train": n_train, "epochs": epochs, "a_max": a_max}
     t0 = time.perf_counter()
     if bootstrap and tuple(bootstrap) != tuple(grid):
         coarse, cinfo = build_surrogate(n_boot, tuple(bootstrap), boot_epochs, batch, lr,
-                                        max_steps=boot_max_steps, tol=tol, log=log)
+                                        max_steps=boot_max_steps, tol=tol, log=log, a_max=a_max)
         info["bootstrap"] = cinfo
         ics, _ = predicted_ics(coarse, train_p, grid, coarse.floor)
         del coarse  # its device buffers go back to the allocator

@@ -68,11 +68,13 @@ class SweepParams:
         return np.array([self.amp, self.beta, self.vz, self.a])
 
 
-def sweep_params(i: int, grids=SWEEP_GRIDS) -> SweepParams:
+def sweep_params(i: int, grids=SWEEP_GRIDS, a_max: float = 0.2) -> SweepParams:
+    """Draw i of the sweep box; a_max widens the wall-amplitude range (the
+    serving mix's large channel has a = 0.3, outside the sweep box)."""
     rng = np.random.default_rng(i)
     L, M = grids[int(rng.integers(len(grids)))]
     amp = float(rng.uniform(0.5, 2.0))
     beta = float(math.exp(rng.uniform(math.log(0.05), math.log(1.0))))
     vz = float(rng.uniform(0.05, 0.3))
-    a = float(rng.uniform(0.0, 0.2))
+    a = float(rng.uniform(0.0, a_max))
     return SweepParams(L, M, amp, beta, vz, a)
