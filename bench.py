@@ -76,6 +76,11 @@ def parse():
                     help="warmstart: generate the training data warm from a surrogate first "
                          "trained on this coarser grid (e.g. 100x40)")
     ap.add_argument("--n-boot", type=int, default=2000)
+    ap.add_argument("--a-max", type=float, default=0.2,
+                    help="surrogate draws: wall amplitude range [0, a_max]")
+    ap.add_argument("--error-grid", type=str, default="",
+                    help="serve: also measure the warm start's distance to the cold steady "
+                         "state on this grid (e.g. 800x320) at a = 0.3")
     ap.add_argument("--plain-sample", type=int, default=32,
                     help="warmstart: solves of the plain march timed one after another")
     ap.add_argument("--warm-fraction", type=float, default=1.0,
@@ -400,6 +405,7 @@ def run_ours(args, rank, world, local_rank):
             "residual_kernel": {"kernel": "residual_kernel", "ms": resid_ms,
                                 "achieved": resid_gbs, "unit": "GB/s", "peak": hbm,
                                 "frac": resid_gbs / hbm,
+                                "traffic": profiled_traffic("residual_kernel")[0],
                                 "alg_bytes_per_launch": RESID_BYTES_PER_CELL * CELLS,
                                 "how": "30 back-to-back launches between two CUDA events"},
             "cpu_baseline": cpu,
@@ -494,32 +500,40 @@ def run_serve(args):
     """The serving mix, bounded: a large converging-diverging
     channel warm-started from the surrogate (coarse prediction remapped on
     the device) in one persistent launch beside small sweep solves admitted by
-    a device-memory budget; the same mix cold for comparison."""
+    a device-memory budget; the same mix cold for comparison.  With
+    --error-grid, the per-field distance to the cold steady state on a large
+    grid where that state is reachable.  Without --surrogate a surrogate is
+    first built on --grid from draws whose wall amplitude reaches --a-max
+    (the large channel's a = 0.3 lies outside the sweep box)."""
     import __graft_entry__
     pkg = __graft_entry__.load_package()
     WS = pkg.warmstart
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    info = {}
     if args.surrogate:
         tr = WS.Trained.load(args.surrogate)
     else:
         L, M = (int(v) for v in args.grid.split("x"))
-        params = WS.draws(range(args.n_train), (L, M))
-        data = WS.solve_all(params, max_steps=args.max_steps)
-        keep = [i for i in range(len(params)) if data.converged[i]]
-        g = WS.grid_of(params[0].config())
-        import numpy as np
-        X = np.stack([WS.inputs_of(params[i], g) for i in keep])
-        Y = np.stack([data.fields[i].reshape(-1, 8) for i in keep])
-        tr = WS.train(X, Y, L, M + 1, epochs=args.epochs, log=log)
+        tr, info = WS.build_surrogate(args.n_train, (L, M), args.epochs,
+                                      max_steps=args.max_steps, log=log,
+                                      save=args.save or None, a_max=args.a_max)
+        info.pop("losses", None)
     bL, bM = (int(v) for v in args.big.split("x"))
     res = pkg.serve.run_serving(tr, big=(bL, bM), n_small=args.n_solves,
                                 max_steps=min(args.max_steps, args.steps), log=log)
+    err = None
+    if args.error_grid:
+        eL, eM = (int(v) for v in args.error_grid.split("x"))
+        err = pkg.serve.large_grid_error(tr, (eL, eM), cap=min(args.max_steps, args.steps),
+                                         log=log)
     return {"metric": "serving mix: small solves/s beside a warm-started large grid",
             "value": res["warm"]["small_solves_per_s"], "unit": "solves/s",
             "higher_is_better": True, "n_gpus": 1, "dtype": "f64", "vs_baseline": None,
             "data": "synthetic (sweep-box draws)",
             "config": {"workload": f"large channel {args.big} a=0.3 + {args.n_solves} small",
-                       "steps_cap": min(args.max_steps, args.steps)}, **res}
+                       "steps_cap": min(args.max_steps, args.steps),
+                       "surrogate_a_max": info.get("a_max")},
+            "surrogate": info, **res, "large_grid_error": err}
 
 
 def run_surrogate(args):

@@ -3,6 +3,14 @@ warm-started from the surrogate's coarse prediction, remapped onto its grid
 by the device bilinear remap, running in the same persistent cooperative
 launch as a batch of small uneven solves admitted by a device-memory budget.
 
+large_grid_error measures what the warm start is worth against the plain
+method's steady state on a large converging-diverging channel whose cold
+steady state is reachable (the 4096 x 1600 one needs ~4 L^2 = 67M steps):
+per-field relative L-inf distance to the cold-started steady state of the
+surrogate's remapped prediction, of the warm run after a serving cap of
+steps, and of the warm run converged; the cold run's own distance after the
+same cap for comparison.
+
 The large solve gets a team of `big_blocks` blocks; the small ones are
 admitted in draw order while their estimated device bytes fit the budget
 (free device memory x `budget_frac`, less the large solve), and take the
@@ -116,3 +124,57 @@ def run_serving(tr: WS.Trained, big: tuple[int, int] = (4096, 1600), a_big: floa
             s.close()
     return {"big_grid": f"{big[0]}x{big[1]}", "a_big": a_big, "n_small_admitted": len(small_p),
             "budget_gib": budget / 2**30, "remap_s": remap_s, "max_steps": max_steps, **out}
+
+
+def large_grid_error(tr: WS.Trained, grid: tuple[int, int] = (800, 320), a_big: float = 0.3,
+                     cap: int = 20_000, max_steps: int = 8_000_000, tol: float = 1e-8,
+                     log=print) -> dict:
+    """See the module docstring.  Both runs use the graph engine with the
+    residual every 50 steps; the warm one starts at the CFL dt of the
+    remapped prediction, the cold one at the workload's dt0."""
+    L, M = grid
+    p = SweepParams(L, M, 1.0, 0.1, 0.1, a_big)
+    cfg = p.config()
+
+    def fields(solver):
+        return WS.fields_of(solver.physical(), L, M)
+
+    cold = build_case(cfg, precision="fast")
+    c1 = cold.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=cap, residual_tol=tol,
+                  residual_every=50)
+    cold_cap = fields(cold)
+    c2 = cold.run(T=1e300, dt=c1.dt, adaptive=True, max_steps=max_steps - c1.steps,
+                  residual_tol=tol, residual_every=50)
+    ref = fields(cold)
+    cold.close()
+    log(f"cold {L}x{M} a={a_big}: converged={c2.converged} after {c1.steps + c2.steps} steps, "
+        f"residual {c2.residual:.2e}")
+    ic = upsampled_ic(tr, p, cfg)
+    pred = WS.fields_of(ic, L, M)
+    warm = GpuSolver(cfg, WS.grid_of(cfg), ic, precision="fast")
+    w1 = warm.run(T=1e300, dt=0.0, adaptive=True, max_steps=cap, residual_tol=tol,
+                  residual_every=50)
+    warm_cap = fields(warm)
+    w2 = warm.run(T=1e300, dt=w1.dt, adaptive=True, max_steps=max_steps - w1.steps,
+                  residual_tol=tol, residual_every=50)
+    warm_conv = fields(warm)
+    warm.close()
+    log(f"warm: converged={w2.converged} after {w1.steps + w2.steps} steps")
+
+    def per_field(x):
+        return dict(zip(S.FIELDS, WS.relative_linf(x, ref).tolist()))
+
+    return {
+        "grid": f"{L}x{M}", "a": a_big, "tol": tol, "cap_steps": cap,
+        "cold_steps": int(c1.steps + c2.steps), "cold_converged": bool(c2.converged),
+        "cold_device_s": (c1.device_ms + c2.device_ms) * 1e-3,
+        "warm_steps": int(w1.steps + w2.steps), "warm_converged": bool(w2.converged),
+        "warm_device_s": (w1.device_ms + w2.device_ms) * 1e-3,
+        "residual_at_cap": {"cold": c1.residual, "warm": w1.residual},
+        "rel_linf_vs_cold_steady": {
+            "prediction": per_field(pred),
+            "warm_at_cap": per_field(warm_cap),
+            "cold_at_cap": per_field(cold_cap),
+            "warm_converged": per_field(warm_conv),
+        },
+    }
