@@ -103,7 +103,7 @@ class Normalizer:
     @classmethod
     def fit(cls, fields: np.ndarray) -> "Normalizer":
         f = fields.reshape(-1, N_OUT)
-        mean, std = f.mean(0), f.std(0)
+        mean, std = f.mean(0, dtype=np.float64), f.std(0, dtype=np.float64)
         const = std <= 1e-12 * np.maximum(1.0, np.abs(mean))
         return cls(mean, np.where(const, 1.0, std), const)
 

@@ -225,7 +225,7 @@ class Trained:
         floor = self.floor if self.floor is not None else np.zeros(2)
         np.savez(path, H=self.net.H, W=self.net.W, mean=self.norm.mean, std=self.norm.std,
                  const=self.norm.const, losses=np.array(self.losses), floor=floor,
-                 **{f"p_{k}": v for k, v in p.items()})
+                 **{f"p_{k}": v.astype(np.float32) for k, v in p.items()})
 
     @classmethod
     def load(cls, path, batch: int = 16) -> "Trained":
@@ -350,16 +350,20 @@ def build_surrogate(n_train=2000, grid=(100, 40), epochs=40, batch=16, lr=1e-3,
     keep = np.flatnonzero(data.converged)
     log(f"training solves on {L}x{M}: {len(keep)} of {n_train} converged, {gen_s:.1f} s")
     g0 = grid_of(train_p[0].config())
-    X = np.stack([inputs_of(train_p[i], g0) for i in keep])
-    Y = np.stack([data.fields[i].reshape(H * W, S.N_OUT) for i in keep])
+    # single precision on the host too: 2000 fine-grid states are GBs
+    X = np.stack([inputs_of(train_p[i], g0).astype(np.float32) for i in keep])
+    Y = np.stack([data.fields[i].reshape(H * W, S.N_OUT).astype(np.float32) for i in keep])
+    data_steps_median = float(np.median(data.steps))
+    data_device_s = data.device_ms * 1e-3
+    del data
     tr = train(X, Y, H, W, epochs=epochs, batch=batch, lr=lr, log=log)
     tr.floor = np.array([0.05 * np.min(Y[..., 0]), 0.05 * np.min(Y[..., 4])])
     log(f"trained {epochs} epochs in {tr.train_s:.1f} s, final loss {tr.losses[-1]:.3e}")
     if save:
         tr.save(save)
     info.update({"n_train_converged": int(len(keep)), "data_gen_s": gen_s,
-                 "data_steps_median": float(np.median(data.steps)),
-                 "data_device_s": data.device_ms * 1e-3, "train_s": tr.train_s,
+                 "data_steps_median": data_steps_median,
+                 "data_device_s": data_device_s, "train_s": tr.train_s,
                  "final_loss": tr.losses[-1], "losses": tr.losses})
     return tr, info
 
