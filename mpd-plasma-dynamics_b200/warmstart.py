@@ -59,6 +59,11 @@ def inputs_of(p: SweepParams, grid: Grid) -> np.ndarray:
     return S.features(S.param_vector(p.amp, p.beta, p.vz, p.a), r, z)
 
 
+def own_inputs(p: SweepParams) -> np.ndarray:
+    """The network input of draw p on its own grid and wall."""
+    return inputs_of(p, grid_of(p.config()))
+
+
 def fields_of(phys10: np.ndarray, L: int, M: int) -> np.ndarray:
     """H x W x 8 network fields from the 10 physical planes."""
     return np.stack([phys10[k, 1:L + 1, 1:M + 2] for k in PLANE_OF_FIELD], axis=-1)
@@ -196,9 +201,8 @@ def predicted_ics(tr: "Trained", params: list[SweepParams], grid, floor) -> tupl
     the prediction is interpolated bilinearly."""
     L, M = grid
     Hs, Ws = tr.net.H, tr.net.W
-    src_grid = (Hs, Ws - 1)
-    g = grid_of(draws([0], src_grid)[0].config())
-    X = np.stack([inputs_of(p, g) for p in params])
+    X = np.stack([own_inputs(SweepParams(Hs, Ws - 1, p.amp, p.beta, p.vz, p.a))
+                  for p in params])
     pred, infer_s = predict(tr, X)
     out = []
     for p, f in zip(params, pred):
@@ -349,9 +353,9 @@ def build_surrogate(n_train=2000, grid=(100, 40), epochs=40, batch=16, lr=1e-3,
     gen_s = time.perf_counter() - t0
     keep = np.flatnonzero(data.converged)
     log(f"training solves on {L}x{M}: {len(keep)} of {n_train} converged, {gen_s:.1f} s")
-    g0 = grid_of(train_p[0].config())
-    # single precision on the host too: 2000 fine-grid states are GBs
-    X = np.stack([inputs_of(train_p[i], g0).astype(np.float32) for i in keep])
+    # single precision on the host too: 2000 fine-grid states are GBs; each
+    # draw's r(z, y) from its own wall (its a)
+    X = np.stack([own_inputs(train_p[i]).astype(np.float32) for i in keep])
     Y = np.stack([data.fields[i].reshape(H * W, S.N_OUT).astype(np.float32) for i in keep])
     data_steps_median = float(np.median(data.steps))
     data_device_s = data.device_ms * 1e-3
