@@ -12,6 +12,7 @@
 // std::runtime_error, like the reference's constructors.
 #pragma once
 
+#include <cstdio>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -21,6 +22,7 @@
 #include "grid.hpp"
 #include "mpd_b200.h"
 #include "mpi_manager.hpp"
+#include "verification.hpp"
 
 class GpuSolver {
 public:
@@ -101,6 +103,40 @@ public:
         return c;
     }
     void SavePrev() { Check(mpd_save_prev(h_)); }
+
+    /// Verification::ComputeIntegrals (src/verification.cpp:16-45) of the device state.
+    Verification::ConservedIntegrals ComputeIntegrals() {
+        double q[7];
+        Check(mpd_integrals(h_, q));
+        Verification::ConservedIntegrals c;
+        c.mass = q[0];
+        c.momentum_z = q[1];
+        c.momentum_r = q[2];
+        c.momentum_phi = q[3];
+        c.energy = q[4];
+        c.mag_flux_z = q[5];
+        c.mag_flux_phi = q[6];
+        return c;
+    }
+
+    /// Diagnostics::CheckCfl (src/diagnostics.cpp:112-125) of the device state:
+    /// the same warning, printed under the same condition.
+    void CheckCfl(double dt, int step_count) {
+        double speed = 0.0;
+        Check(mpd_max_wave_speed(h_, &speed));
+        const double dx = cfg_.dz < cfg_.dy ? cfg_.dz : cfg_.dy;
+        const double dt_max = cfg_.cfl_number * dx / (speed + 1.0e-10);
+        if (dt > dt_max && step_count % 1000 == 0)
+            std::printf("WARNING [step %d]: dt=%.6e exceeds CFL limit dt_max=%.6e "
+                        "(max_speed=%.3f, CFL=%.2f)\n",
+                        step_count, dt, dt_max, speed, dt / dt_max * cfg_.cfl_number);
+    }
+
+    /// The physical values of one global cell (rho, v_z, v_r, v_phi, e, p, P,
+    /// H_z, H_r, H_phi), e.g. the driver's checkpoint cell (src/main.cpp:258-270).
+    void Probe(int l_global, int m_global, double out10[10]) {
+        Check(mpd_probe(h_, l_global, m_global, out10));
+    }
 
     /// Copy the device state into the host Fields (u0_*, u_* and the physical arrays).
     void Download() {

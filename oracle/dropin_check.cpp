@@ -168,6 +168,33 @@ int main(int argc, char **argv) {
               Same(fc.e, fg.e, "e") && Same(fc.p, fg.p, "p") && Same(fc.P, fg.P, "P") &&
               Same(fc.H_z, fg.H_z, "H_z") && Same(fc.H_r, fg.H_r, "H_r") &&
               Same(fc.H_phi, fg.H_phi, "H_phi");
+    // the driver's 1000-step report through GpuSolver: the integrals
+    // (Verification::ComputeIntegrals, sums in another order: 1e-13) and the
+    // checkpoint cell (bit for bit)
+    const Verification::ConservedIntegrals ic_c = Verification::ComputeIntegrals(fc, grid, cfg, mpi);
+    const Verification::ConservedIntegrals ic_g = gpu.ComputeIntegrals();
+    const double qc[7] = {ic_c.mass, ic_c.momentum_z, ic_c.momentum_r, ic_c.momentum_phi,
+                          ic_c.energy, ic_c.mag_flux_z, ic_c.mag_flux_phi};
+    const double qg[7] = {ic_g.mass, ic_g.momentum_z, ic_g.momentum_r, ic_g.momentum_phi,
+                          ic_g.energy, ic_g.mag_flux_z, ic_g.mag_flux_phi};
+    for (int k = 0; k < 7; ++k)
+        if (std::abs(qc[k] - qg[k]) > 1e-13 * std::abs(qc[k])) {
+            std::printf("MISMATCH integral %d: %.17g vs %.17g\n", k, qc[k], qg[k]);
+            ok = false;
+        }
+    if (L > 20 && M >= 40) {
+        double q[10];
+        gpu.Probe(20, 40, q);
+        const double want[5] = {fc.rho[21][41], fc.v_z[21][41], fc.v_phi[21][41], fc.e[21][41],
+                                fc.H_phi[21][41]};
+        const double got[5] = {q[0], q[1], q[3], q[4], q[9]};
+        for (int k = 0; k < 5; ++k)
+            if (got[k] != want[k]) {
+                std::printf("MISMATCH probe %d: %.17g vs %.17g\n", k, got[k], want[k]);
+                ok = false;
+            }
+    }
+    gpu.CheckCfl(dt_g, steps);
     std::printf("%s after %d steps of %dx%d (dt=%.17g)\n", ok ? "DROPIN OK" : "DROPIN FAIL", steps,
                 L, M, dt_c);
     return ok ? 0 : 1;
