@@ -4,17 +4,25 @@
 //   C[b](m, n) = alpha * sum_k bf16(A[b](m, k)) * bf16(B[b](n, k)) + beta * C[b](m, n)
 //
 // A, B and C are FP32 in global memory with arbitrary element strides (so a
-// transposed operand costs nothing extra); operands are rounded to BF16 as
-// they are staged in shared memory, products accumulate in FP32 in tensor
-// memory (TMEM).  One CTA of 4 warps computes a 128 x 64 tile of C:
-//   * warp 0 allocates 64 TMEM columns (the 128 x 64 FP32 accumulator);
-//   * per 64-wide K chunk every thread converts its share of the A (128 x 64)
-//     and B (64 x 64) tiles into the canonical K-major, no-swizzle layout of
-//     8 x 16-byte core matrices, then one thread issues four
-//     tcgen05.mma.cta_group::1.kind::f16 (M 128, N 64, K 16) from shared-
-//     memory descriptors and commits them to an mbarrier (bounded wait);
-//   * the epilogue reads the accumulator with tcgen05.ld (each warp its 32
-//     TMEM lanes = 32 rows of C) and writes alpha * acc + beta * C.
+// transposed operand costs nothing extra); operands are rounded to BF16 in
+// shared memory, products accumulate in FP32 in tensor memory (TMEM).  One
+// CTA of 4 warps computes a 128 x 64 tile of C through a software pipeline
+// over 32-wide K chunks:
+//   * copies: the FP32 tiles of chunk k + 2 are fetched into a 3-stage
+//     shared-memory ring with 16-byte cp.async copies (zero-filled past the
+//     operand's edge) while chunk k is converted and chunk k - 1 multiplied;
+//     an operand whose K or M/N direction is contiguous and 16-byte aligned
+//     is copied as it lies (K-major rows or MN-major rows), any other one
+//     element by element;
+//   * conversion: every thread rounds its share of chunk k to BF16 and
+//     writes it in the canonical K-major, no-swizzle layout of 8 x 16-byte
+//     core matrices (double-buffered);
+//   * MMA: one thread issues two tcgen05.mma.cta_group::1.kind::f16
+//     (M 128, N 64, K 16) per chunk from shared-memory descriptors and
+//     commits them to an mbarrier (bounded wait before the buffer is reused);
+//   * warp 0 allocates 64 TMEM columns (the 128 x 64 FP32 accumulator); the
+//     epilogue reads it with tcgen05.ld (each warp its 32 TMEM lanes = 32
+//     rows of C) and writes alpha * acc + beta * C.
 // Shared-memory descriptor and instruction-descriptor fields follow the
 // sm100 UMMA descriptors (start address >> 4 in bits 0-13, leading byte
 // offset >> 4 in 16-29, stride byte offset >> 4 in 32-45, version 1 in
@@ -42,14 +50,22 @@ using mpd::smem_addr;
 
 constexpr int kTileM = 128;
 constexpr int kTileN = 64;
-constexpr int kTileK = 64;
+constexpr int kTileK = 32;          // K per pipeline chunk (two MMAs of K 16)
+constexpr int kSplitUnit = 64;      // split-K spans are multiples of this
 constexpr int kGemmThreads = 128;
+constexpr int kCopyStages = 3;      // FP32 chunks in flight per CTA
 constexpr uint32_t kTmemCols = 64;
 
-// Bytes of the core-matrix layouts: A tile = 8 K-chunks x 16 row groups,
-// B tile = 8 K-chunks x 8 row groups, 128 bytes per core matrix.
+// Bytes of the BF16 core-matrix layouts: A tile = 4 K-chunks x 16 row
+// groups, B tile = 4 K-chunks x 8 row groups, 128 bytes per core matrix.
 constexpr int kABytes = kTileM * kTileK * 2;
 constexpr int kBBytes = kTileN * kTileK * 2;
+// FP32 staging of one chunk: K-major tiles as [row][32 k + 4 padding] (the
+// padding spreads a warp's 16-byte reads of consecutive rows over all
+// banks), MN-major tiles as [k][rows].
+constexpr int kKPad = kTileK + 4;
+constexpr int kA32 = (kTileM * kKPad > kTileK * kTileM) ? kTileM * kKPad : kTileK * kTileM;
+constexpr int kB32 = (kTileN * kKPad > kTileK * kTileN) ? kTileN * kKPad : kTileK * kTileN;
 
 __device__ int g_gemm_wait_fail = 0;
 
@@ -108,55 +124,104 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return *reinterpret_cast<uint32_t *>(&h);
 }
 
-// Stage rows [r0, r0 + ROWS) x k [k0, k1) of an operand into the core-matrix
-// layout: chunk c (8 k) of row group g at (c * ROWS/8 + g) * 128 bytes, row
-// r & 7 at 16 (r & 7), element e at 2 e.  All of a thread's loads are issued
-// before any is converted; rows with 16-byte aligned K-contiguous data take
-// two float4 loads per 8 elements.
+// 16-byte asynchronous copy global -> shared; bytes past src_bytes (0..16)
+// are zero-filled, and with src_bytes == 0 nothing is read.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+                 "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// How an operand's FP32 tile is staged: rows of K (K contiguous in memory),
+// rows of M or N (those contiguous), or element by element.
+enum StageMode { kKMajor = 0, kMNMajor = 1, kScalar = 2 };
+
+__device__ __forceinline__ int stage_mode(const float *base, long long s_rows, long long s_k) {
+    const bool aligned = ((uintptr_t)base & 15) == 0;
+    if (s_k == 1 && aligned && (s_rows % 4) == 0) return kKMajor;
+    if (s_rows == 1 && aligned && (s_k % 4) == 0) return kMNMajor;
+    return kScalar;
+}
+
+// Fetch rows [r0, r0 + ROWS) x k [k0, k0 + 32) of an operand into FP32
+// staging: kKMajor as [row][kKPad], kMNMajor and kScalar as [k][ROWS rows].
+// Past nrows or k1 the values are zero.  kScalar loads synchronously.
 template <int ROWS>
-__device__ __forceinline__ void stage(unsigned char *dst, const float *base, long long sr,
-                                      long long sk, int nrows, int k1, int r0, int k0,
-                                      bool vec) {
-    constexpr int kUnits = ROWS * (kTileK / 8);
-    constexpr int kPer = kUnits / kGemmThreads;
-    const bool k_contig = sk == 1;
-    float f[kPer][8];
+__device__ __forceinline__ void fetch(float *dst, const float *base, long long sr, long long sk,
+                                      int nrows, int k1, int r0, int k0, int mode) {
+    if (mode == kKMajor) {
+        constexpr int kChunks = ROWS * (kTileK / 4);
 #pragma unroll
-    for (int i = 0; i < kPer; ++i) {
-        const int u = threadIdx.x + i * kGemmThreads;
-        const int rl = k_contig ? (u >> 3) : (u % ROWS);
-        const int c = k_contig ? (u & 7) : (u / ROWS);
-        const int r = r0 + rl, k = k0 + 8 * c;
-        const float *p = base + (long long)r * sr + (long long)k * sk;
-        if (r < nrows && k + 8 <= k1 && vec) {
-            const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
-            const float4 b = __ldg(reinterpret_cast<const float4 *>(p) + 1);
-            f[i][0] = a.x; f[i][1] = a.y; f[i][2] = a.z; f[i][3] = a.w;
-            f[i][4] = b.x; f[i][5] = b.y; f[i][6] = b.z; f[i][7] = b.w;
-        } else {
+        for (int i = 0; i < kChunks / kGemmThreads; ++i) {
+            const int u = threadIdx.x + i * kGemmThreads;
+            const int rl = u / (kTileK / 4), c = u % (kTileK / 4);
+            const int r = r0 + rl, k = k0 + 4 * c;
+            const int valid = (r < nrows && k < k1) ? 4 * min(4, k1 - k) : 0;
+            const float *src = valid ? base + (long long)r * sr + k : base;
+            cp_async16(smem_addr(dst + rl * kKPad + 4 * c), src, valid);
+        }
+    } else if (mode == kMNMajor) {
+        constexpr int kChunks = kTileK * (ROWS / 4);
 #pragma unroll
-            for (int e = 0; e < 8; ++e)
-                f[i][e] = (r < nrows && k + e < k1) ? __ldg(p + (long long)e * sk) : 0.0f;
+        for (int i = 0; i < kChunks / kGemmThreads; ++i) {
+            const int u = threadIdx.x + i * kGemmThreads;
+            const int kl = u / (ROWS / 4), c = u % (ROWS / 4);
+            const int k = k0 + kl, r = r0 + 4 * c;
+            const int valid = (k < k1 && r < nrows) ? 4 * min(4, nrows - r) : 0;
+            const float *src = valid ? base + (long long)k * sk + r : base;
+            cp_async16(smem_addr(dst + kl * ROWS + 4 * c), src, valid);
+        }
+    } else {
+#pragma unroll 4
+        for (int u = threadIdx.x; u < ROWS * kTileK; u += kGemmThreads) {
+            const int kl = u / ROWS, rl = u % ROWS;
+            const int r = r0 + rl, k = k0 + kl;
+            dst[kl * ROWS + rl] =
+                (r < nrows && k < k1) ? __ldg(base + (long long)r * sr + (long long)k * sk) : 0.0f;
         }
     }
+}
+
+// Round the FP32 staging of a chunk to BF16 in the K-major core-matrix
+// layout: 8-k chunk c of row group g at (c * ROWS/8 + g) * 128 bytes, row
+// r & 7 at 16 (r & 7), element e at 2 e.
+template <int ROWS>
+__device__ __forceinline__ void convert(unsigned char *dst, const float *src, int mode) {
+    constexpr int kUnits = ROWS * (kTileK / 8);
 #pragma unroll
-    for (int i = 0; i < kPer; ++i) {
+    for (int i = 0; i < kUnits / kGemmThreads; ++i) {
         const int u = threadIdx.x + i * kGemmThreads;
-        const int rl = k_contig ? (u >> 3) : (u % ROWS);
-        const int c = k_contig ? (u & 7) : (u / ROWS);
+        const int rl = u % ROWS, c = u / ROWS;  // consecutive threads: consecutive rows
+        float f[8];
+        if (mode == kKMajor) {
+            const float4 a = *reinterpret_cast<const float4 *>(src + rl * kKPad + 8 * c);
+            const float4 b = *reinterpret_cast<const float4 *>(src + rl * kKPad + 8 * c + 4);
+            f[0] = a.x; f[1] = a.y; f[2] = a.z; f[3] = a.w;
+            f[4] = b.x; f[5] = b.y; f[6] = b.z; f[7] = b.w;
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) f[e] = src[(8 * c + e) * ROWS + rl];
+        }
         uint4 v;
-        v.x = pack_bf16(f[i][0], f[i][1]);
-        v.y = pack_bf16(f[i][2], f[i][3]);
-        v.z = pack_bf16(f[i][4], f[i][5]);
-        v.w = pack_bf16(f[i][6], f[i][7]);
+        v.x = pack_bf16(f[0], f[1]);
+        v.y = pack_bf16(f[2], f[3]);
+        v.z = pack_bf16(f[4], f[5]);
+        v.w = pack_bf16(f[6], f[7]);
         *reinterpret_cast<uint4 *>(dst + (c * (ROWS / 8) + (rl >> 3)) * 128 + (rl & 7) * 16) = v;
     }
 }
 
-// Two stages of tiles in dynamic shared memory (48 KB per block): the tiles
-// of chunk k+1 are staged while the tensor core works on chunk k.
+// Dynamic shared memory: the FP32 staging ring, then two BF16 buffers.
+constexpr int kStage32Bytes = (kA32 + kB32) * 4;
 constexpr int kStageBytes = kABytes + kBBytes;
-constexpr int kGemmSmem = 2 * kStageBytes;
+constexpr int kGemmSmem = kCopyStages * kStage32Bytes + 2 * kStageBytes;
 
 // C tile (m0, n0) of batch b over K range [k_begin, k_end).  With ksplit > 1
 // the raw FP32 sums go to work (split s of batch b: dense M x N at
@@ -173,8 +238,10 @@ __global__ void __launch_bounds__(kGemmThreads) nn_gemm_kernel(const mpd_gemm_de
     const int k_end = min(d.K, k_begin + kspan);
     const float *A = d.A + (long long)b * d.sab;
     const float *B = d.B + (long long)b * d.sbb;
-    const bool vec_a = d.sak == 1 && (d.sam % 4) == 0 && ((uintptr_t)A & 15) == 0;
-    const bool vec_b = d.sbk == 1 && (d.sbn % 4) == 0 && ((uintptr_t)B & 15) == 0;
+    const int mode_a = stage_mode(A, d.sam, d.sak);
+    const int mode_b = stage_mode(B, d.sbn, d.sbk);
+    float *ring = reinterpret_cast<float *>(gemm_smem);
+    unsigned char *bf = gemm_smem + kCopyStages * kStage32Bytes;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -193,38 +260,57 @@ __global__ void __launch_bounds__(kGemmThreads) nn_gemm_kernel(const mpd_gemm_de
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
 
-    bool ok = true;
     const int nchunks = k_end > k_begin ? (k_end - k_begin + kTileK - 1) / kTileK : 0;
+    auto fetch_chunk = [&](int kc) {
+        float *st = ring + (kc % kCopyStages) * (kA32 + kB32);
+        const int k0 = k_begin + kc * kTileK;
+        fetch<kTileM>(st, A, d.sam, d.sak, d.M, k_end, m0, k0, mode_a);
+        fetch<kTileN>(st + kA32, B, d.sbn, d.sbk, d.N, k_end, n0, k0, mode_b);
+    };
+    // prologue: chunks 0 .. kCopyStages-2 in flight, one commit group each
+#pragma unroll
+    for (int kc = 0; kc < kCopyStages - 1; ++kc) {
+        if (kc < nchunks) fetch_chunk(kc);
+        cp_async_commit();
+    }
+    bool ok = true;
     for (int kc = 0; kc < nchunks; ++kc) {
+        // the stage chunk kc + 2 lands in held chunk kc - 1, converted last iteration
+        if (kc + kCopyStages - 1 < nchunks) fetch_chunk(kc + kCopyStages - 1);
+        cp_async_commit();
+        cp_async_wait<kCopyStages - 1>();   // this thread's copies of chunk kc are in
         const int buf = kc & 1;
-        unsigned char *sA = gemm_smem + buf * kStageBytes;
-        unsigned char *sB = sA + kABytes;
         if (kc >= 2) {
-            // the MMAs of chunk kc - 2 read this stage: wait for their commit
+            // the MMAs of chunk kc - 2 read this BF16 buffer: wait for their commit
             const bool arrived = mbar_wait_bounded(smem_addr(&bar[buf]), ((kc - 2) >> 1) & 1);
             ok = __syncthreads_and(arrived);
             if (!ok) break;
+        } else {
+            __syncthreads();
         }
-        const int k0 = k_begin + kc * kTileK;
-        stage<kTileM>(sA, A, d.sam, d.sak, d.M, k_end, m0, k0, vec_a);
-        stage<kTileN>(sB, B, d.sbn, d.sbk, d.N, k_end, n0, k0, vec_b);
+        const float *st = ring + (kc % kCopyStages) * (kA32 + kB32);
+        unsigned char *sA = bf + buf * kStageBytes;
+        unsigned char *sB = sA + kABytes;
+        convert<kTileM>(sA, st, mode_a);
+        convert<kTileN>(sB, st + kA32, mode_b);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (threadIdx.x == 0) {
             tc_fence_after();
             const uint32_t a_addr = smem_addr(sA), b_addr = smem_addr(sB);
 #pragma unroll
-            for (int s = 0; s < kTileK / 16; ++s) {
-                // K slice s = core-matrix chunks 2s, 2s+1
-                const uint64_t ad = smem_desc(a_addr + s * 2 * (kTileM / 8) * 128,
+            for (int s2 = 0; s2 < kTileK / 16; ++s2) {
+                // K slice s2 = core-matrix chunks 2 s2, 2 s2 + 1
+                const uint64_t ad = smem_desc(a_addr + s2 * 2 * (kTileM / 8) * 128,
                                               (kTileM / 8) * 128, 128);
-                const uint64_t bd = smem_desc(b_addr + s * 2 * (kTileN / 8) * 128,
+                const uint64_t bd = smem_desc(b_addr + s2 * 2 * (kTileN / 8) * 128,
                                               (kTileN / 8) * 128, 128);
-                mma_bf16(tmem, ad, bd, (kc > 0 || s > 0) ? 1u : 0u);
+                mma_bf16(tmem, ad, bd, (kc > 0 || s2 > 0) ? 1u : 0u);
             }
             mma_commit(smem_addr(&bar[buf]));
         }
     }
+    cp_async_wait<0>();  // no copy may still land after the CTA exits
     if (ok && nchunks > 0) {
         // commits complete in order: the last one covers every MMA
         const int last = nchunks - 1;
@@ -309,16 +395,17 @@ int mpd_nn_gemm(const mpd_gemm_desc *d, void *stream) {
     const long long tiles = (long long)((d->M + kTileM - 1) / kTileM) *
                             ((d->N + kTileN - 1) / kTileN) * d->batch;
     int ksplit = 1;
-    if (d->work && tiles < 296 && d->K >= 4 * kTileK) {
+    if (d->work && tiles < 296 && d->K >= 4 * kSplitUnit) {
         long long want = (296 + tiles - 1) / tiles;
-        const long long by_k = d->K / (2 * kTileK);
+        const long long by_k = d->K / (2 * kSplitUnit);
         const long long by_room = d->work_floats / ((long long)d->M * d->N * d->batch);
         want = want < by_k ? want : by_k;
         want = want < by_room ? want : by_room;
         want = want < 64 ? want : 64;
         if (want > 1) ksplit = (int)want;
     }
-    const int kspan = ((d->K + ksplit - 1) / ksplit + kTileK - 1) / kTileK * kTileK;
+    const int kspan =
+        ((d->K + ksplit - 1) / ksplit + kSplitUnit - 1) / kSplitUnit * kSplitUnit;
     ksplit = (d->K + kspan - 1) / kspan;
     if ((long long)d->batch * ksplit > 65535) {
         mpd::SetLastError("mpd_nn_gemm: batch too large for one launch");
