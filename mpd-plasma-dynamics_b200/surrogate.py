@@ -167,6 +167,8 @@ class SpectralOperator:
         # split-K partial sums of the long-K products (grid sums, weight gradients)
         self.work = torch.zeros(16 * batch * self.Q * WIDTH, **f32)
         self.loss = torch.zeros(1, device=dev, dtype=torch.float64)
+        self.target = torch.zeros(rows, N_OUT, **f32)   # the captured iteration's targets
+        self.graph = None
         self.step = 0
         self.lib = N.load()
 
@@ -299,6 +301,39 @@ class SpectralOperator:
         # lift (the input needs no gradient)
         self._wgrad(self.x, N_IN, gh, Cw, g["W_in"])
         self._colsum(gh, g["b_in"])
+
+    # ------------------------------------------------------ captured iteration
+    def capture(self) -> None:
+        """Record forward, loss (against self.target) and backward of one
+        training iteration as a CUDA graph: ~100 kernel launches replayed as
+        one.  Inputs and targets are read from self.x and self.target, so a
+        step only refills those buffers; Adam stays outside the graph (its
+        bias correction takes the step count as an argument)."""
+        torch = self.torch
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):  # one eager pass first (one-time set-up of the launches)
+            self.forward()
+            self.loss_and_grad(self.target)
+            self.backward()
+        torch.cuda.current_stream().wait_stream(side)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.forward()
+            self.loss_and_grad(self.target)
+            self.backward()
+        self.graph = g
+
+    def train_step(self, lr=1e-3) -> None:
+        """One training iteration on self.x / self.target: the captured graph
+        when there is one, else the same calls eagerly; then Adam."""
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self.forward()
+            self.loss_and_grad(self.target)
+            self.backward()
+        self.adam_step(lr=lr)
 
     def adam_step(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
         self.step += 1

@@ -258,18 +258,16 @@ def train(X: np.ndarray, Y: np.ndarray, H: int, W: int, epochs: int = 40, batch:
     t0 = time.perf_counter()
     total = epochs * nb
     it = 0
+    net.capture()   # forward + loss + backward replayed as one CUDA graph
     for ep in range(epochs):
         perm = torch.from_numpy(rng.permutation(N)[:nb * batch]).to(dev)
         ep_loss = 0.0
         for b in range(nb):
             idx = perm[b * batch:(b + 1) * batch]
             net.x.copy_(dX.index_select(0, idx).reshape(-1, S.N_IN))
-            tgt = dY.index_select(0, idx).reshape(-1, S.N_OUT)
-            net.forward()
-            net.loss_and_grad(tgt)
-            net.backward()
+            net.target.copy_(dY.index_select(0, idx).reshape(-1, S.N_OUT))
             rate = lr * 0.5 * (1 + math.cos(math.pi * it / total)) + 1e-5
-            net.adam_step(lr=rate)
+            net.train_step(lr=rate)
             ep_loss += float(net.loss.cpu()[0]) if b == nb - 1 else 0.0
             it += 1
         losses.append(ep_loss)
