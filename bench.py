@@ -53,14 +53,16 @@ def parse():
                          "kernel (lf_pair_kernel) on the final state")
     ap.add_argument("--precision", choices=("fast", "exact"), default="fast")
     ap.add_argument("--workload", choices=("plain", "warmstart", "batch", "surrogate", "serve",
-                                           "converge"),
+                                           "converge", "sweep"),
                     default="plain",
                     help="plain: the 1600x640 time step (default); warmstart: surrogate-warm-"
                          "started batched steady solves vs the plain time march; batch: the "
                          "batched sweep of uneven grids; surrogate: training iterations of "
                          "the warm-start network; serve: a large warm-started grid beside a "
                          "memory-budgeted batch of small solves; converge: the 1600x640 "
-                         "channel time-marched to an L-inf residual of 1e-8 (--max-steps)")
+                         "channel time-marched to an L-inf residual of 1e-8 (--max-steps); "
+                         "sweep: the uneven sweep cold, surrogate-warm (--surrogate) and by the "
+                         "plain march one solve after another")
     ap.add_argument("--n-train", type=int, default=2000)
     ap.add_argument("--n-eval", type=int, default=256)
     ap.add_argument("--epochs", type=int, default=60)
@@ -555,6 +557,28 @@ def run_serve(args):
             "surrogate": info, **res, "large_grid_error": err}
 
 
+def run_sweep(args):
+    """The north star's comparison on the parameter sweep of uneven grids:
+    batched cold, batched surrogate-warm (--surrogate, trained on a coarse
+    grid and interpolated onto each draw's grid) and the plain FP64 march one
+    solve after another (--plain-sample of the draws), all capped at
+    --max-steps.  value = warm batch solves/s."""
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    WS = pkg.warmstart
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    tr = WS.Trained.load(args.surrogate)
+    res = WS.sweep_comparison(tr, args.n_solves, args.max_steps, plain_sample=args.plain_sample,
+                              log=log)
+    return {"metric": "steady solves/s, warm-start batch on the uneven sweep",
+            "value": res["warm_batch_solves_per_s"], "unit": "solves/s",
+            "higher_is_better": True, "n_gpus": 1, "dtype": "f64 solver, bf16/f32 surrogate",
+            "data": "synthetic (sweep-box draws, numpy default_rng(i))", "vs_baseline": None,
+            "config": {"workload": "sweep grids {100x40,200x80,400x160,800x320}",
+                       "n_solves": args.n_solves, "max_steps": args.max_steps,
+                       "surrogate": args.surrogate}, **res}
+
+
 def run_surrogate(args):
     """Training iterations of the warm-start network (forward, MSE, backward,
     Adam) on random inputs: grid --grid, batch 16; --warmup untimed, --steps
@@ -754,7 +778,8 @@ def main():
     if args.workload != "plain":
         if rank == 0:
             runner = {"warmstart": run_warmstart, "surrogate": run_surrogate,
-                      "serve": run_serve, "converge": run_converge}[args.workload]
+                      "serve": run_serve, "converge": run_converge,
+                      "sweep": run_sweep}[args.workload]
             line = runner(args)
             print(json.dumps(line))
         return

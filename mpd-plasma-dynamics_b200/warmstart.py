@@ -196,16 +196,17 @@ def solve_warm(params: list[SweepParams], ics: list, max_steps=200_000, tol=1e-8
 
 def predicted_ics(tr: "Trained", params: list[SweepParams], grid, floor) -> tuple[list, float]:
     """Initial planes predicted by the surrogate for each draw on `grid`
-    (None where the prediction is not finite) and the inference seconds.  A
-    surrogate trained on another (coarser) grid predicts on its own grid and
-    the prediction is interpolated bilinearly."""
-    L, M = grid
+    (None: each draw's own grid) — None where the prediction is not finite —
+    and the inference seconds.  A surrogate trained on another (coarser)
+    grid predicts on its own grid and the prediction is interpolated
+    bilinearly."""
     Hs, Ws = tr.net.H, tr.net.W
     X = np.stack([own_inputs(SweepParams(Hs, Ws - 1, p.amp, p.beta, p.vz, p.a))
                   for p in params])
     pred, infer_s = predict(tr, X)
     out = []
     for p, f in zip(params, pred):
+        L, M = grid if grid is not None else (p.L, p.M)
         f = f.reshape(Hs, Ws, S.N_OUT)
         if not np.all(np.isfinite(f)):
             out.append(None)
@@ -458,3 +459,68 @@ def run_pipeline(n_train=2000, n_eval=256, grid=(100, 40), epochs=40, batch=16, 
     res = evaluate(tr, n_eval, grid, max_steps, tol, plain_sample, warm_fraction, tight_tol,
                    tight_sample, log)
     return {**info, **res}
+
+
+def sweep_comparison(tr: Trained, n: int = 256, max_steps: int = 200_000, tol: float = 1e-8,
+                     plain_sample: int = 32, log=print) -> dict:
+    """The sweep of uneven grids (workloads.sweep_params(i), i < n) solved
+    three ways, all capped at max_steps: the batched engine from the
+    workload's initial condition (cold), the batched engine from the
+    surrogate's prediction interpolated onto each draw's grid (warm, judged
+    and backed by the plain march: solve_warm with the full cap as budget),
+    and the plain FP64 march one solve after another on the first
+    plain_sample draws.  Rates count all solves and converged solves."""
+    params = [sweep_params(i) for i in range(n)]
+    floor = tr.floor if tr.floor is not None else np.zeros(2)
+    ics, infer_s = predicted_ics(tr, params, None, floor)
+    cold = solve_all(params, max_steps=max_steps, tol=tol)
+    warm, fell = solve_warm(params, ics, max_steps=max_steps, tol=tol, budget=max_steps)
+    log(f"sweep of {n}: cold converged {int(cold.converged.sum())} in "
+        f"{cold.device_ms / 1e3:.1f} s, warm converged {int(warm.converged.sum())} in "
+        f"{warm.device_ms / 1e3:.1f} s ({int(fell.sum())} fell back)")
+    seq_ms, seq_conv = 0.0, 0
+    for p in params[:plain_sample]:
+        cfg = p.config()
+        sv = build_case(cfg, precision="fast")
+        r = sv.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=max_steps, residual_tol=tol,
+                   residual_every=50, engine="graph")
+        seq_ms += r.device_ms
+        seq_conv += int(r.converged)
+        sv.close()
+    both = cold.converged & warm.converged
+    agree = [relative_linf(warm.fields[i], cold.fields[i]) for i in np.flatnonzero(both)]
+    by_grid = {}
+    for i, p in enumerate(params):
+        d = by_grid.setdefault(f"{p.L}x{p.M}", {"n": 0, "cold_converged": 0,
+                                                 "warm_converged": 0, "cold_steps": [],
+                                                 "warm_steps": []})
+        d["n"] += 1
+        d["cold_converged"] += int(cold.converged[i])
+        d["warm_converged"] += int(warm.converged[i])
+        d["cold_steps"].append(int(cold.steps[i]))
+        d["warm_steps"].append(int(warm.steps[i]))
+    for d in by_grid.values():
+        d["cold_steps_median"] = float(np.median(d.pop("cold_steps")))
+        d["warm_steps_median"] = float(np.median(d.pop("warm_steps")))
+    cold_s = cold.device_ms * 1e-3
+    warm_s = warm.device_ms * 1e-3 + infer_s
+    seq_s = seq_ms * 1e-3
+    return {
+        "n": n, "max_steps": max_steps, "tol": tol, "plain_sample": plain_sample,
+        "cold_batch_s": cold_s, "warm_batch_s": warm_s, "plain_sample_s": seq_s,
+        "cold_converged": int(cold.converged.sum()), "warm_converged": int(warm.converged.sum()),
+        "plain_sample_converged": seq_conv, "warm_fallbacks": int(fell.sum()),
+        "cold_batch_solves_per_s": n / cold_s, "warm_batch_solves_per_s": n / warm_s,
+        "plain_solves_per_s": plain_sample / seq_s if seq_s > 0 else None,
+        "cold_batch_converged_per_s": int(cold.converged.sum()) / cold_s,
+        "warm_batch_converged_per_s": int(warm.converged.sum()) / warm_s,
+        "plain_converged_per_s": seq_conv / seq_s if seq_s > 0 else None,
+        "warm_over_plain": (n / warm_s) / (plain_sample / seq_s) if seq_s > 0 else None,
+        "warm_vs_cold_state_rel_linf_max": np.stack(agree).max(0).tolist() if agree else None,
+        "warm_p50_ms": float(np.percentile(warm.solve_ms, 50)),
+        "warm_p99_ms": float(np.percentile(warm.solve_ms, 99)),
+        "cold_p50_ms": float(np.percentile(cold.solve_ms, 50)),
+        "cold_p99_ms": float(np.percentile(cold.solve_ms, 99)),
+        "surrogate_inference_s": infer_s,
+        "by_grid": by_grid,
+    }
