@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--n-boot", type=int, default=2000)
     ap.add_argument("--a-max", type=float, default=0.2,
                     help="surrogate draws: wall amplitude range [0, a_max]")
+    ap.add_argument("--error-a", type=str, default="0.3,0.2",
+                    help="serve: wall amplitudes of the --error-grid channels")
     ap.add_argument("--error-grid", type=str, default="",
                     help="serve: also measure the warm start's distance to the cold steady "
                          "state on this grid (e.g. 800x320) at a = 0.3")
@@ -545,8 +547,9 @@ def run_serve(args):
     err = None
     if args.error_grid:
         eL, eM = (int(v) for v in args.error_grid.split("x"))
-        err = pkg.serve.large_grid_error(tr, (eL, eM), cap=min(args.max_steps, args.steps),
-                                         log=log)
+        err = [pkg.serve.large_grid_error(tr, (eL, eM), a_big=float(a),
+                                          cap=min(args.max_steps, args.steps), log=log)
+               for a in args.error_a.split(",")]
     return {"metric": "serving mix: small solves/s beside a warm-started large grid",
             "value": res["warm"]["small_solves_per_s"], "unit": "solves/s",
             "higher_is_better": True, "n_gpus": 1, "dtype": "f64", "vs_baseline": None,
