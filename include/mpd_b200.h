@@ -309,7 +309,10 @@ int mpd_batch_capacity(mpd_batch *b, int *blocks);
  * dt0 (n entries, or NULL for p->dt): each solve's initial dt (<= 0: the CFL
  * limit of its state).  stats: n entries.  solve_ms (n entries, or NULL): time from the first step
  * any solve took in this run to this solve's last step.  device_ms (or NULL):
- * the whole run. */
+ * the whole run.  The plan holds while every team has work; between launches,
+ * once fewer solves are left than teams, the remaining solves are re-planned
+ * one per team with the wave's blocks split evenly between them (results do
+ * not depend on the plan, only the time does). */
 int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *team_blocks,
                   const int *solve_team, const double *dt0, mpd_run_stats *stats,
                   double *solve_ms, double *device_ms);

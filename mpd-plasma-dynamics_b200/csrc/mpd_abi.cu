@@ -1473,9 +1473,10 @@ int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *
 
     MPD_CK(cudaEventRecord(b->ev0, b->stream));
     long long last = -1;
+    int nteams_cur = nteams, blocks_cur = blocks;
     for (;;) {
-        MPD_CK(cudaMemsetAsync(b->d_gs, 0, nteams * sizeof(mpd::GridSync), b->stream));
-        MPD_CK(mpd::launch_lf_batch(blocks, ba, b->stream));
+        MPD_CK(cudaMemsetAsync(b->d_gs, 0, nteams_cur * sizeof(mpd::GridSync), b->stream));
+        MPD_CK(mpd::launch_lf_batch(blocks_cur, ba, b->stream));
         long long total = 0;
         bool all_done = true, failed = false;
         for (mpd_solver *s : b->solvers)
@@ -1493,6 +1494,49 @@ int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *
         if (all_done) break;
         if (total == last) return Fail(MPD_ERR_TIMEOUT, "batch run made no progress");
         last = total;
+        // Elastic re-plan: once fewer solves are left than teams (the rest
+        // would idle for the remaining launches), every remaining solve gets
+        // a team of its own and the wave's blocks are split evenly between
+        // them, up to the blocks that still give it interior tasks (64 at
+        // most: beyond that the team barriers cost more than the tasks
+        // give).  A solve's results do not depend on its team's size.
+        std::vector<int> active;
+        for (int i = 0; i < n; ++i)
+            if (!b->solvers[i]->h_st->done) active.push_back(i);
+        if (!active.empty() && static_cast<int>(active.size()) < nteams_cur) {
+            nteams_cur = static_cast<int>(active.size());
+            const int share = b->capacity / nteams_cur;
+            std::vector<int> tf(nteams_cur + 1, 0), sf(nteams_cur + 1, 0);
+            for (int k = 0; k < nteams_cur; ++k) {
+                mpd_solver *sv = b->solvers[active[k]];
+                const int strips = (sv->M + mpd::kFastCells - 1) / mpd::kFastCells;
+                const long long tasks = static_cast<long long>(strips) * sv->L;
+                int want = static_cast<int>((tasks + mpd::kTmaWarps - 1) / mpd::kTmaWarps);
+                want = want < 64 ? want : 64;
+                int nb = share < want ? share : want;
+                if (nb < 1) nb = 1;
+                tf[k + 1] = tf[k] + nb;
+                sf[k + 1] = k + 1;
+                int nstrips = 0, nbands = 0;
+                mpd::persist_tasks(sv->g, nb, nstrips, nbands);
+                args[active[k]].nstrips = nstrips;
+                args[active[k]].nbands = nbands;
+            }
+            std::vector<int> ints2;
+            ints2.insert(ints2.end(), tf.begin(), tf.end());
+            ints2.insert(ints2.end(), sf.begin(), sf.end());
+            ints2.insert(ints2.end(), active.begin(), active.end());
+            MPD_CK(cudaMemcpyAsync(b->d_solves, args.data(), n * sizeof(mpd::PersistArgs),
+                                   cudaMemcpyHostToDevice, b->stream));
+            MPD_CK(cudaMemcpyAsync(b->d_ints, ints2.data(), ints2.size() * sizeof(int),
+                                   cudaMemcpyHostToDevice, b->stream));
+            MPD_CK(cudaStreamSynchronize(b->stream));
+            ba.team_first = b->d_ints;
+            ba.solve_first = b->d_ints + (nteams_cur + 1);
+            ba.order = b->d_ints + 2 * (nteams_cur + 1);
+            ba.nteams = nteams_cur;
+            blocks_cur = tf[nteams_cur];
+        }
     }
     MPD_CK(cudaEventRecord(b->ev1, b->stream));
     MPD_CK(cudaEventSynchronize(b->ev1));

@@ -22,7 +22,8 @@
 //     commits them to an mbarrier (bounded wait before the buffer is reused);
 //   * warp 0 allocates 64 TMEM columns (the 128 x 64 FP32 accumulator); the
 //     epilogue reads it with tcgen05.ld (each warp its 32 TMEM lanes = 32
-//     rows of C) and writes alpha * acc + beta * C.
+//     rows of C) into shared memory and writes alpha * acc + beta * C along
+//     C's contiguous direction (whole 128-byte lines per warp).
 // Shared-memory descriptor and instruction-descriptor fields follow the
 // sm100 UMMA descriptors (start address >> 4 in bits 0-13, leading byte
 // offset >> 4 in 16-29, stride byte offset >> 4 in 32-45, version 1 in
@@ -318,9 +319,13 @@ __global__ void __launch_bounds__(kGemmThreads) nn_gemm_kernel(const mpd_gemm_de
     }
     tc_fence_after();
     if (ok) {
-        const int m = m0 + warp * 32 + lane;
-        float *C = d.C + (long long)b * d.scb;
-        float *W = ksplit > 1 ? d.work + ((long long)split * d.batch + b) * d.M * d.N : nullptr;
+        // The accumulator through shared memory (the copy ring is free now):
+        // tcgen05.ld gives each thread one row of the tile; the tile is then
+        // written along C's contiguous direction, so a warp's stores (and,
+        // with beta != 0, its loads of C) are whole 128-byte lines.
+        float *T = ring;              // kTileM x kTilePad floats
+        constexpr int kTilePad = kTileN + 1;   // odd stride: conflict-free rows and columns
+        const int row = warp * 32 + lane;
 #pragma unroll
         for (int j = 0; j < kTileN / 16; ++j) {
             float v[16];
@@ -330,17 +335,40 @@ __global__ void __launch_bounds__(kGemmThreads) nn_gemm_kernel(const mpd_gemm_de
 #pragma unroll
                 for (int i = 0; i < 16; ++i) v[i] = 0.0f;
             }
-            if (m < d.M) {
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const int n = n0 + 16 * j + i;
-                    if (n >= d.N) continue;
+            for (int i = 0; i < 16; ++i) T[row * kTilePad + 16 * j + i] = v[i];
+        }
+        __syncthreads();
+        float *C = d.C + (long long)b * d.scb;
+        float *W = ksplit > 1 ? d.work + ((long long)split * d.batch + b) * d.M * d.N : nullptr;
+        if (W || d.scn == 1 || d.scm != 1) {
+            // lanes along n: rows of C (or of the dense partials) are contiguous
+            for (int r = warp; r < kTileM; r += kGemmThreads / 32) {
+                const int m = m0 + r;
+                if (m >= d.M) break;
+                for (int cc = lane; cc < kTileN; cc += 32) {
+                    const int n = n0 + cc;
+                    if (n >= d.N) break;
+                    const float v = T[r * kTilePad + cc];
                     if (W) {
-                        W[(long long)m * d.N + n] = v[i];
+                        W[(long long)m * d.N + n] = v;
                     } else {
                         float *c = C + (long long)m * d.scm + (long long)n * d.scn;
-                        *c = d.beta == 0.0f ? d.alpha * v[i] : d.alpha * v[i] + d.beta * *c;
+                        *c = d.beta == 0.0f ? d.alpha * v : d.alpha * v + d.beta * *c;
                     }
+                }
+            }
+        } else {
+            // lanes along m: columns of C are contiguous
+            for (int cc = warp; cc < kTileN; cc += kGemmThreads / 32) {
+                const int n = n0 + cc;
+                if (n >= d.N) break;
+                for (int r = lane; r < kTileM; r += 32) {
+                    const int m = m0 + r;
+                    if (m >= d.M) break;
+                    const float v = T[r * kTilePad + cc];
+                    float *c = C + (long long)m * d.scm + (long long)n * d.scn;
+                    *c = d.beta == 0.0f ? d.alpha * v : d.alpha * v + d.beta * *c;
                 }
             }
         }
