@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--n-boot", type=int, default=2000)
     ap.add_argument("--a-max", type=float, default=0.2,
                     help="surrogate draws: wall amplitude range [0, a_max]")
+    ap.add_argument("--skip-mix", action="store_true",
+                    help="serve: only the --error-grid measurements, not the serving mix")
     ap.add_argument("--error-a", type=str, default="0.3,0.2",
                     help="serve: wall amplitudes of the --error-grid channels")
     ap.add_argument("--error-grid", type=str, default="",
@@ -542,8 +544,9 @@ def run_serve(args):
                                       save=args.save or None, a_max=args.a_max)
         info.pop("losses", None)
     bL, bM = (int(v) for v in args.big.split("x"))
-    res = pkg.serve.run_serving(tr, big=(bL, bM), n_small=args.n_solves,
-                                max_steps=min(args.max_steps, args.steps), log=log)
+    res = {} if args.skip_mix else pkg.serve.run_serving(
+        tr, big=(bL, bM), n_small=args.n_solves, max_steps=min(args.max_steps, args.steps),
+        log=log)
     err = None
     if args.error_grid:
         eL, eM = (int(v) for v in args.error_grid.split("x"))
@@ -551,7 +554,7 @@ def run_serve(args):
                                           cap=min(args.max_steps, args.steps), log=log)
                for a in args.error_a.split(",")]
     return {"metric": "serving mix: small solves/s beside a warm-started large grid",
-            "value": res["warm"]["small_solves_per_s"], "unit": "solves/s",
+            "value": res["warm"]["small_solves_per_s"] if res else None, "unit": "solves/s",
             "higher_is_better": True, "n_gpus": 1, "dtype": "f64", "vs_baseline": None,
             "data": "synthetic (sweep-box draws)",
             "config": {"workload": f"large channel {args.big} a=0.3 + {args.n_solves} small",
