@@ -341,34 +341,69 @@ __global__ void __launch_bounds__(kGemmThreads) nn_gemm_kernel(const mpd_gemm_de
         __syncthreads();
         float *C = d.C + (long long)b * d.scb;
         float *W = ksplit > 1 ? d.work + ((long long)split * d.batch + b) * d.M * d.N : nullptr;
+        // In both directions a warp takes 8 rows (or columns) at a time and
+        // issues all its loads of C before any store: a store to C and a
+        // later load of C are not reordered, so one element at a time would
+        // serialise on the memory latency.  Every element of C is read and
+        // written by one thread only, so its loads may use the read-only path.
+        constexpr int kBatch = 8;
         if (W || d.scn == 1 || d.scm != 1) {
             // lanes along n: rows of C (or of the dense partials) are contiguous
-            for (int r = warp; r < kTileM; r += kGemmThreads / 32) {
-                const int m = m0 + r;
-                if (m >= d.M) break;
-                for (int cc = lane; cc < kTileN; cc += 32) {
-                    const int n = n0 + cc;
-                    if (n >= d.N) break;
-                    const float v = T[r * kTilePad + cc];
-                    if (W) {
-                        W[(long long)m * d.N + n] = v;
-                    } else {
-                        float *c = C + (long long)m * d.scm + (long long)n * d.scn;
-                        *c = d.beta == 0.0f ? d.alpha * v : d.alpha * v + d.beta * *c;
+            for (int r0 = warp; r0 < kTileM; r0 += kBatch * (kGemmThreads / 32)) {
+                float cin[kBatch][kTileN / 32];
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j) {
+#pragma unroll
+                    for (int h2 = 0; h2 < kTileN / 32; ++h2) {
+                        const int m = m0 + r0 + j * (kGemmThreads / 32);
+                        const int n = n0 + lane + 32 * h2;
+                        cin[j][h2] = (!W && d.beta != 0.0f && m < d.M && n < d.N)
+                                         ? __ldg(C + (long long)m * d.scm + (long long)n * d.scn)
+                                         : 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j) {
+#pragma unroll
+                    for (int h2 = 0; h2 < kTileN / 32; ++h2) {
+                        const int r = r0 + j * (kGemmThreads / 32), cc = lane + 32 * h2;
+                        const int m = m0 + r, n = n0 + cc;
+                        if (m >= d.M || n >= d.N) continue;
+                        const float v = T[r * kTilePad + cc];
+                        if (W)
+                            W[(long long)m * d.N + n] = v;
+                        else
+                            C[(long long)m * d.scm + (long long)n * d.scn] =
+                                d.alpha * v + d.beta * cin[j][h2];
                     }
                 }
             }
         } else {
             // lanes along m: columns of C are contiguous
-            for (int cc = warp; cc < kTileN; cc += kGemmThreads / 32) {
-                const int n = n0 + cc;
-                if (n >= d.N) break;
-                for (int r = lane; r < kTileM; r += 32) {
-                    const int m = m0 + r;
-                    if (m >= d.M) break;
-                    const float v = T[r * kTilePad + cc];
-                    float *c = C + (long long)m * d.scm + (long long)n * d.scn;
-                    *c = d.beta == 0.0f ? d.alpha * v : d.alpha * v + d.beta * *c;
+            for (int c0 = warp; c0 < kTileN; c0 += kBatch * (kGemmThreads / 32)) {
+                float cin[kBatch][kTileM / 32];
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j) {
+#pragma unroll
+                    for (int h2 = 0; h2 < kTileM / 32; ++h2) {
+                        const int n = n0 + c0 + j * (kGemmThreads / 32);
+                        const int m = m0 + lane + 32 * h2;
+                        cin[j][h2] = (d.beta != 0.0f && m < d.M && n < d.N)
+                                         ? __ldg(C + (long long)m * d.scm + (long long)n * d.scn)
+                                         : 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j) {
+#pragma unroll
+                    for (int h2 = 0; h2 < kTileM / 32; ++h2) {
+                        const int cc = c0 + j * (kGemmThreads / 32), r = lane + 32 * h2;
+                        const int m = m0 + r, n = n0 + cc;
+                        if (m >= d.M || n >= d.N) continue;
+                        const float v = T[r * kTilePad + cc];
+                        C[(long long)m * d.scm + (long long)n * d.scn] =
+                            d.alpha * v + d.beta * cin[j][h2];
+                    }
                 }
             }
         }
