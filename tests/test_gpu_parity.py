@@ -447,3 +447,23 @@ def test_blowup_is_flagged_nonfinite(pkg, precision, engine):
         rg = g.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=5000, engine="graph")
         assert rg.steps == res.steps
         g.close()
+
+
+def test_profiling_launches_leave_the_run_unchanged(pkg):
+    """mpd_profile_kernel (back-to-back timing launches of the interior kernels
+    and the residual pass) between two runs: the run that follows ends in
+    the same bits, dt and t as one never interrupted."""
+    case = cases.channel_case(L=200, M=80, a=0.1)
+    cfg = case.cfg
+    a = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+    b = pkg.GpuSolver(cfg, case.grid, case.phys, precision="fast")
+    ra = a.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=30)
+    rb = b.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=30)
+    for which in ("interior", "interior_pair", "residual"):
+        assert b.profile_kernel(which, 5, rb.dt) > 0.0
+    ra = a.run(T=1e300, dt=ra.dt, adaptive=True, max_steps=40)
+    rb = b.run(T=1e300, dt=rb.dt, adaptive=True, max_steps=40)
+    assert (ra.t, ra.dt) == (rb.t, rb.dt)
+    np.testing.assert_array_equal(a.conserved(), b.conserved())
+    a.close()
+    b.close()
