@@ -232,6 +232,21 @@ int mpd_set_physical(mpd_solver *s, const double *phys10);
 int mpd_set_expression_ic(mpd_solver *s, const char *const exprs[8], int n_vars,
                           const char *const *var_names, const double *var_values);
 
+/* Where a fast step's boundary ring runs (new; no reference counterpart: the
+ * reference applies the faces after the central update, src/solver.cpp:
+ * 22-37, and both forms keep that order of values).  on = 1: beside the
+ * interior kernel, in bc_overlap_kernel, which recomputes the
+ * central cells the faces read from the step's input state, so the ring's
+ * dependent chains overlap the interior and only the end-of-step controller
+ * waits for it; the interior kernel then computes rows 2..L-1.  on = 0 (the
+ * default): after the interior kernel, reading the central cells it stored.  The two give
+ * the same bits.  Takes effect from the next step; exact precision, the first
+ * step and grids with L_max < 4 always use the second form.
+ * mpd_ring_overlap_active reports whether fast steps of the handle use the
+ * first. */
+int mpd_set_ring_overlap(mpd_solver *s, int on);
+int mpd_ring_overlap_active(mpd_solver *s, int *active);
+
 /* The handle's CUDA stream (a cudaStream_t), for callers that time or order
  * work around the solver. */
 int mpd_get_stream(mpd_solver *s, void **stream);

@@ -137,6 +137,8 @@ SIGNATURES = [
     ("mpd_set_expression_ic", C.c_int, [_VP, C.POINTER(C.c_char_p), C.c_int,
                                         C.POINTER(C.c_char_p), DP]),
     ("mpd_get_stream", C.c_int, [_VP, C.POINTER(_VP)]),
+    ("mpd_set_ring_overlap", C.c_int, [_VP, C.c_int]),
+    ("mpd_ring_overlap_active", C.c_int, [_VP, C.POINTER(C.c_int)]),
     ("mpd_device_bytes", C.c_int, [_VP, C.POINTER(C.c_size_t)]),
     ("mpd_profile_kernels", C.c_int, [_VP, C.c_int, C.c_double, DP]),
     ("mpd_profile_kernel", C.c_int, [_VP, C.c_int, C.c_int, C.c_double, DP]),

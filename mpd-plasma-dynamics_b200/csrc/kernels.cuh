@@ -172,8 +172,8 @@ __device__ __forceinline__ void prefetch_l1(const void *p) {
 }
 
 // Ahead of bc_ring_final's dependent chain for cell (l, m), touch the lines it
-// may read so that its loads hit this SM's L1: the central and wall line
-// entries next to the cell, the wall profiles of its rows and, on the axis
+// may read so that its loads hit this SM's L1: the central (unless they are
+// recomputed) and wall line entries next to the cell, the wall profiles of its rows and, on the axis
 // column, the u0 values of AxisLF.  A hint only: no value depends on it.
 __device__ __forceinline__ void ring_prefetch(const BcView &v, int l, int m) {
     const Geo &g = v.g;
@@ -186,8 +186,10 @@ __device__ __forceinline__ void ring_prefetch(const BcView &v, int l, int m) {
     if (m == 1 || m == M + 1) {
         const int line = m == 1 ? 2 : 3;  // central column 2 or M
         const int wl = m == 1 ? 0 : 1;    // wall column 1 or M+1
+        if (!v.recompute) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) prefetch_l1(v.cphys + (size_t)(line * 8 + k) * len + l);
+            for (int k = 0; k < 8; ++k) prefetch_l1(v.cphys + (size_t)(line * 8 + k) * len + l);
+        }
 #pragma unroll
         for (int k = 0; k < 10; ++k) prefetch_l1(v.wphys + (size_t)(wl * 10 + k) * len + l);
         if (m == 1) {
@@ -202,8 +204,10 @@ __device__ __forceinline__ void ring_prefetch(const BcView &v, int l, int m) {
         }
     } else {
         const int line = l == 1 ? 0 : 1;  // central row 2 or L-1
+        if (!v.recompute) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) prefetch_l1(v.cphys + (size_t)(line * 8 + k) * len + m);
+            for (int k = 0; k < 8; ++k) prefetch_l1(v.cphys + (size_t)(line * 8 + k) * len + m);
+        }
         if (m <= 2 || m >= M) {
             const int row = l == 1 ? 2 : L - 1;
 #pragma unroll
@@ -454,6 +458,69 @@ __global__ void MPD_BC_BOUNDS bc_kernel(Geo g, double *buf0, double *buf1,
     if (flags) cs.flush(st);
     if (MPD_PDL_TRIG_BC == 2) pdl_trigger();
     if (last_block_arrived(st)) step_controller(g, st, step, dt, flags);
+}
+
+// The boundary ring of a fast step run beside the interior kernel instead of
+// after it (the interior launched just before, lf_tma_kernel<.., true>, which
+// writes rows 2..L-1 only and lets this kernel start at once).  Every value
+// the faces need from this step's central update is recomputed from the
+// input state (BcView::recompute), so nothing here waits for the interior:
+// the ring's dependent chains (several microseconds of loads, face
+// evaluations and reconstructions per cell) overlap the interior instead of
+// following it.  Blocks of one warp at most 128 registers fit beside three
+// interior blocks of an SM; a grid of at most one block per SM strides over
+// the ring slots.  Only the controller needs the interior's wave-speed
+// maximum: the last ring block to finish waits for the interior to complete
+// (pdl_wait), then runs it.  The state read before that wait was written by
+// the previous step's controller, which completed before the interior
+// launched; it is read through L2.  Exited blocks count as having let the
+// next kernel in; the last one does so once the interior has completed.
+#ifndef MPD_OVERLAP_MAXNREG
+#define MPD_OVERLAP_MAXNREG 128
+#endif
+__global__ void __maxnreg__(MPD_OVERLAP_MAXNREG)
+    bc_overlap_kernel(Geo g, double *buf0, double *buf1, const double *__restrict__ ic,
+                      BcTable bc, DevState *st, double dt_arg, int use_state_dt, double *wall0,
+                      double *wall1, int len) {
+    extern __shared__ __align__(16) unsigned char bc_smem_raw[];
+    {
+        const int4 *src = reinterpret_cast<const int4 *>(bc.seg);
+        int4 *dst = reinterpret_cast<int4 *>(bc_smem_raw);
+        const int n = bc.nseg_total * (int)(sizeof(SegDesc) / sizeof(int4));
+        for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
+        __syncthreads();
+        bc.seg = reinterpret_cast<const SegDesc *>(bc_smem_raw);
+    }
+    if (__ldcg(&st->done)) return;
+    const long long step = __ldcg(&st->step);
+    const double *u0 = (step & 1) ? buf1 : buf0;
+    double *u = (step & 1) ? buf0 : buf1;
+    const double dt = use_state_dt ? __ldcg(&st->dt) : dt_arg;
+    const int flags = __ldcg(&st->want_ws) ? kFlagWs : 0;
+    BcView v = make_bc_view(g, u0, u, ic, nullptr, (step & 1) ? wall1 : wall0, len, step == 0,
+                            1, dt, bc);
+    v.recompute = 1;
+    double *wnext = (step & 1) ? wall0 : wall1;
+    CellStats cs;
+    cs.init();
+    const int n = ring_count(g);
+    const int stride = (int)(gridDim.x * blockDim.x);
+    for (int i = (int)(blockIdx.x * blockDim.x + threadIdx.x); i < n; i += stride)
+        ring_cell_update(v, i, wnext, (flags & kFlagWs) != 0, cs);
+    if (flags) cs.flush(st);
+    if (!last_block_arrived(st)) return;
+    pdl_wait();
+    // every interior block has retired: the next step's interior is placed
+    // on a free GPU (all its blocks at once, spread over the SMs) while this
+    // controller runs
+    pdl_trigger();
+    if (__ldcg(&st->done)) {
+        // the interior gave up on a bounded wait and stopped the run: the
+        // step is not taken
+        st->arrive = 0u;
+        return;
+    }
+    step_controller(g, st, step, dt, flags);
 }
 
 // L-inf residual of the step that just finished (new; the reference has only

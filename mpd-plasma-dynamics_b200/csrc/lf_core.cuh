@@ -582,6 +582,60 @@ MPD_HD bool wants_central(int L, int M, int l, int m) {
     return l == 2 || l == L - 1 || m == 2 || m == M;
 }
 
+// Point (n, p) of the step's input state as the fast interior's warp sees it:
+// conserved values, primitives and radius (ghost rows: U = 0, r = 1, every
+// primitive 0).
+MPD_HD void fast_point(const Geo &g, const double *u0, int n, int p, double gm1, double U[8],
+                       FastPrim &q, double &r) {
+    const bool gh = n <= 0 || n >= g.L + 1 || p > g.M + 1;
+    load_cons(u0, g.ps, g.ix(n, p), U);
+    r = gh ? 1.0 : g.r(n, p);
+    q = fast_prim(U, r, gm1, gh);
+}
+
+// The fast interior's new conserved values of cell (l, m), 1 <= l <= L,
+// 2 <= m <= M, computed on their own from the step's input state u0: the
+// operations of lf_tma_kernel's warp in the same order (A from point row
+// l-1; B from the east and west points' shares, which the warp moves by
+// shuffles, and the point's own sources; closed with point row l+1), so the
+// result is bit-identical to the value that kernel stores for the cell.
+MPD_HD void fast_cell_alone(const Geo &g, const double *u0, double dt, int l, int m,
+                            double out[8]) {
+    const double gm1 = g.gamma - 1.0;
+    const double kz = dt * (0.5 / g.dz);
+    double U[8], Gz[8], A[9], B[9], S[10];
+    FastPrim q;
+    double r;
+    fast_point(g, u0, l - 1, m, gm1, U, q, r);
+    fast_gz(U, q, r, Gz);
+    fast_a(U, Gz, kz, A);
+    const double kr = dt * g.hdr[l];
+    {
+        double Ue[8], Uw[8], Gre[8], Grw[8], re, rw;
+        FastPrim qe, qw;
+        fast_point(g, u0, l, m + 1, gm1, Ue, qe, re);
+        fast_gr(Ue, qe, re, Gre);
+        fast_point(g, u0, l, m - 1, gm1, Uw, qw, rw);
+        fast_gr(Uw, qw, rw, Grw);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const double ce = (k == 7) ? 0.25 * Ue[7] : fma(kr, Gre[k], 0.25 * Ue[k]);
+            const double cw = (k == 7) ? 0.25 * Uw[7] : fma(-kr, Grw[k], 0.25 * Uw[k]);
+            B[k] = ce + cw;
+        }
+        const double d7 = Gre[7] - Grw[7];
+        fast_point(g, u0, l, m, gm1, U, q, r);
+        B[2] = fma(dt, fma(q.rho * q.vphi, q.vphi, q.P) - q.Hphi * q.Hphi, B[2]);
+        B[3] = fma(dt, fma(-q.rho * q.vr, q.vphi, q.Hphi * q.Hr), B[3]);
+        B[4] = fma(-q.p * kr, d7, B[4]);
+        B[8] = q.p;
+    }
+    fast_sum(A, B, S);
+    fast_point(g, u0, l + 1, m, gm1, U, q, r);
+    fast_gz(U, q, r, Gz);
+    fast_finish(S, U, Gz, kz, out);
+}
+
 // Everything one boundary step reads.
 struct BcView {
     Geo g;
@@ -595,6 +649,11 @@ struct BcView {
     int fast;             // MPD_PRECISION_FAST: reconstruct with reciprocals
     double dt;
     BcTable bc;
+    // The faces run beside the fast interior instead of after it: central
+    // cells they read are recomputed from u0 (fast_cell_alone) instead of
+    // read from the central lines, and ring cells no face covers take that
+    // value too (the interior then writes neither).
+    int recompute = 0;
 };
 
 // Fields::UpdatePhysicalFromU of one cell on the boundary path: the exact
@@ -654,6 +713,10 @@ MPD_HD Phys central_phys(const BcView &v, int l, int m) {
     int idx;
     const int line = central_line(v.g.L, v.g.M, l, m, idx);
     double u[8];
+    if (v.recompute) {
+        fast_cell_alone(v.g, v.u0, v.dt, l, m, u);
+        return recon_bc(v, u, v.g.r(l, m));
+    }
     if (line >= 0) {
         const double *b = v.cphys + (size_t)line * 8 * v.len + idx;
 #pragma unroll
@@ -1053,7 +1116,10 @@ MPD_HD void bc_ring_final(const BcView &v, int l, int m, double u[8]) {
         return;
     }
     if (m >= 2 && m <= M) {
-        load_cons(v.u, g.ps, g.ix(l, m), u);
+        if (v.recompute)
+            fast_cell_alone(g, v.u0, v.dt, l, m, u);
+        else
+            load_cons(v.u, g.ps, g.ix(l, m), u);
         return;
     }
     for (int k = 0; k < 8; ++k) u[k] = 0.0;

@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(32 * kPairWarps, MPD_PAIR_MINB)
     int strip, band, nb;
     tma_task(task, nstrips, nbands, nbands_edge, strip, band, nb);
     int l_begin = 1, l_end = 1;
-    if (band < nb) tma_band(g.L, nb, band, l_begin, l_end);
+    if (band < nb) tma_band(1, g.L, nb, band, l_begin, l_end);
     const uint32_t bar0 =
         smem_addr(smem + kPairWarps * kPairStages * kPairRowBytes) + 8u * wib * kPairStages;
     // While the previous kernel of the stream may still run: only this

@@ -269,13 +269,13 @@ __device__ __forceinline__ bool persist_solve(const PersistArgs &a, const CUtens
         for (int task = my_warp; ok && task < ntasks; task += team_warps) {
             const int strip = task % a.nstrips;
             int l_begin, l_end;
-            tma_band(a.g.L, a.nbands, task / a.nstrips, l_begin, l_end);
+            tma_band(1, a.g.L, a.nbands, task / a.nstrips, l_begin, l_end);
             if (l_begin >= l_end) continue;
             tma_warp_setup(w, a.g, strip, par ? a.buf0 : a.buf1, st, a.cphys, a.len, dt,
                            par ? map1 : map0);
             if (lane == 0) fence_proxy_async_global();
             __syncwarp();
-            if (!tma_band_run<true>(w, l_begin, l_end, jrow, ws_key, nf)) ok = false;
+            if (!tma_band_run<true, true>(w, l_begin, l_end, jrow, ws_key, nf)) ok = false;
         }
         {
             unsigned long long key[1] = {ws_key};

@@ -55,10 +55,13 @@ constexpr int kTmaRowBytes = kTmaRow * 8;     // 2048
 // + 128 bytes to align the stages: TMA destinations need 128-byte alignment
 constexpr int kTmaSmem = kTmaWarps * kTmaStages * (kTmaRowBytes + 8) + 128;
 
-// Rows [l_begin, l_end) of band b out of nbands over l = 1..L.
-__host__ __device__ inline void tma_band(int L, int nbands, int b, int &l_begin, int &l_end) {
-    l_begin = 1 + (int)((long long)b * L / nbands);
-    l_end = 1 + (int)((long long)(b + 1) * L / nbands);
+// Rows [l_begin, l_end) of band b out of nbands over the rows first ..
+// first + count - 1 (1..L, or 2..L-1 when the boundary ring runs beside the
+// interior and computes rows 1 and L itself).
+__host__ __device__ inline void tma_band(int first, int count, int nbands, int b, int &l_begin,
+                                         int &l_end) {
+    l_begin = first + (int)((long long)b * count / nbands);
+    l_end = first + (int)((long long)(b + 1) * count / nbands);
 }
 
 // The first and last strips cost more per row than the others (a per-warp
@@ -164,7 +167,7 @@ struct TmaWarp {
 // compiler interleaves them: every lane evaluates the wave speed (halo and
 // ghost lanes too, on whatever their values give) and only output lanes of
 // rows 2..L-1 feed it to the maximum.
-template <bool WANT_WS, bool WITH_POINT>
+template <bool WANT_WS, bool WITH_POINT, bool CENTRAL>
 __device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, uint32_t &j, double A[9],
                                         double S[10], double &r_l, double &ir_l,
                                         unsigned long long &ws_key, unsigned int &nf) {
@@ -190,7 +193,8 @@ __device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, uint32_t &j, do
             s.u[(size_t)k * g.ps + i] = out[k];
 #endif
         }
-        if (wants_central(g.L, g.M, l, s.p)) store_central(s.cphys, s.len, g.L, g.M, l, s.p, out);
+        if (CENTRAL && wants_central(g.L, g.M, l, s.p))
+            store_central(s.cphys, s.len, g.L, g.M, l, s.p, out);
     }
     if (WANT_WS) {
         // The wave speed is positive or NaN / inf, so its bits order like its
@@ -211,7 +215,7 @@ __device__ __forceinline__ bool tma_row(const TmaWarp &w, int l, uint32_t &j, do
 // count (advanced by the l_end - l_begin + 2 rows the band consumes).  Returns
 // false if a row never arrived; the copies still in flight have then been
 // waited for (bounded).
-template <bool WANT_WS>
+template <bool WANT_WS, bool CENTRAL>
 __device__ __forceinline__ bool tma_band_run(TmaWarp &w, int l_begin, int l_end, uint32_t &j,
                                              unsigned long long &ws_key, unsigned int &nf) {
     const FastStrip &s = w.f;
@@ -242,8 +246,8 @@ __device__ __forceinline__ bool tma_band_run(TmaWarp &w, int l_begin, int l_end,
     }
     int l = l_begin;
     for (; ok && l < l_end - 1; ++l)
-        ok = tma_row<WANT_WS, true>(w, l, j, A, S, r_l, ir_l, ws_key, nf);
-    if (ok) ok = tma_row<WANT_WS, false>(w, l, j, A, S, r_l, ir_l, ws_key, nf);
+        ok = tma_row<WANT_WS, true, CENTRAL>(w, l, j, A, S, r_l, ir_l, ws_key, nf);
+    if (ok) ok = tma_row<WANT_WS, false, CENTRAL>(w, l, j, A, S, r_l, ir_l, ws_key, nf);
     if (!ok) {
         if (w.lane == 0) {
             const uint32_t end = w.jbase + (uint32_t)w.nrows;
@@ -287,12 +291,21 @@ __device__ __forceinline__ unsigned char *tma_smem_base(unsigned char *raw) {
     return raw + ((128u - (smem_addr(raw) & 127u)) & 127u);
 }
 
-template <bool WANT_WS>
+// RING_BESIDE: the boundary ring of this step runs in bc_overlap_kernel,
+// launched right after this kernel and running beside it: cell rows 2..L-1
+// only (the ring kernel computes rows 1 and L) and no central lines.
+// early_trigger: the next kernel of the stream is let in as soon as this one
+// has read the step's state (the ring kernel, which must start at once);
+// otherwise once a block's rows are done.  Back-to-back launches of this
+// kernel alone take the latter: a next interior placed block by block as
+// this one's blocks retire would crowd its edge-strip blocks onto the SMs
+// that free first.
+template <bool WANT_WS, bool RING_BESIDE>
 __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
     lf_tma_kernel(Geo g, const __grid_constant__ CUtensorMap map0,
                   const __grid_constant__ CUtensorMap map1, double *buf0, double *buf1,
                   DevState *st, double dt_arg, int use_state_dt, double *cphys, int len,
-                  int nstrips, int nbands, int nbands_edge) {
+                  int nstrips, int nbands, int nbands_edge, int early_trigger) {
     extern __shared__ __align__(128) unsigned char tma_smem_raw[];
     unsigned char *tma_smem = tma_smem_base(tma_smem_raw);
     const int wib = threadIdx.x >> 5;
@@ -300,7 +313,12 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
     int strip, band, nb;
     tma_task(task, nstrips, nbands, nbands_edge, strip, band, nb);
     int l_begin = 1, l_end = 1;
-    if (band < nb) tma_band(g.L, nb, band, l_begin, l_end);
+    if (band < nb) {
+        if (RING_BESIDE)
+            tma_band(2, g.L - 2, nb, band, l_begin, l_end);
+        else
+            tma_band(1, g.L, nb, band, l_begin, l_end);
+    }
     const uint32_t bar0 =
         smem_addr(tma_smem + kTmaWarps * kTmaStages * kTmaRowBytes) + 8u * wib * kTmaStages;
     // While the previous kernel of the stream may still run: only this
@@ -312,7 +330,7 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
         mbar_init_fence();
     }
     pdl_wait();
-    if (MPD_PDL_TRIG_INT == 1) pdl_trigger();
+    if (early_trigger) pdl_trigger();
     if (st->done) return;
     const long long step = st->step;
 
@@ -327,7 +345,8 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
     if (l_begin < l_end) {
         __syncwarp();
         uint32_t j = 0;
-        if (!tma_band_run<WANT_WS>(w, l_begin, l_end, j, ws_key, nf) && w.lane == 0) {
+        if (!tma_band_run<WANT_WS, !RING_BESIDE>(w, l_begin, l_end, j, ws_key, nf) &&
+            w.lane == 0) {
             // a row never arrived: record the failure and stop the run
             atomicExch(&st->wait_fail, 1);
             atomicExch(&st->done, 1);
@@ -337,7 +356,7 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
             }
         }
     }
-    if (MPD_PDL_TRIG_INT == 2) pdl_trigger();
+    if (!early_trigger) pdl_trigger();
     if (WANT_WS) {
         unsigned long long key[1] = {ws_key};
         unsigned long long *dst[1] = {&st->ws_acc};
@@ -354,13 +373,15 @@ inline cudaError_t plan_lf_tma(const Geo &g, int device, TmaPlan &plan) {
     int sms = 0, per_sm = 0;
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(lf_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kTmaSmem);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(lf_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kTmaSmem);
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lf_tma_kernel<true>,
+    void (*const kernels[4])(Geo, const CUtensorMap, const CUtensorMap, double *, double *,
+                             DevState *, double, int, double *, int, int, int, int, int) = {
+        lf_tma_kernel<true, false>, lf_tma_kernel<false, false>, lf_tma_kernel<true, true>,
+        lf_tma_kernel<false, true>};
+    for (auto k : kernels) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem);
+        if (e != cudaSuccess) return e;
+    }
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lf_tma_kernel<true, false>,
                                                       32 * kTmaWarps, kTmaSmem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
@@ -393,14 +414,13 @@ inline cudaError_t plan_lf_tma(const Geo &g, int device, TmaPlan &plan) {
 inline cudaError_t launch_lf_tma(const Geo &g, const TmaPlan &plan, const CUtensorMap &map0,
                                  const CUtensorMap &map1, double *buf0, double *buf1,
                                  DevState *st, double dt, int use_state_dt, bool want_ws,
-                                 double *cphys, int len, cudaStream_t stream) {
-    if (want_ws)
-        return launch_pdl(lf_tma_kernel<true>, dim3(plan.blocks), dim3(32 * kTmaWarps), kTmaSmem,
-                          stream, g, map0, map1, buf0, buf1, st, dt, use_state_dt, cphys, len,
-                          plan.nstrips, plan.nbands, plan.nbands_edge);
-    return launch_pdl(lf_tma_kernel<false>, dim3(plan.blocks), dim3(32 * kTmaWarps), kTmaSmem,
-                      stream, g, map0, map1, buf0, buf1, st, dt, use_state_dt, cphys, len,
-                      plan.nstrips, plan.nbands, plan.nbands_edge);
+                                 bool ring_beside, bool early_trigger, double *cphys, int len,
+                                 cudaStream_t stream) {
+    auto kernel = want_ws ? (ring_beside ? lf_tma_kernel<true, true> : lf_tma_kernel<true, false>)
+                          : (ring_beside ? lf_tma_kernel<false, true> : lf_tma_kernel<false, false>);
+    return launch_pdl(kernel, dim3(plan.blocks), dim3(32 * kTmaWarps), kTmaSmem, stream, g, map0,
+                      map1, buf0, buf1, st, dt, use_state_dt, cphys, len, plan.nstrips,
+                      plan.nbands, plan.nbands_edge, early_trigger ? 1 : 0);
 }
 
 }  // namespace mpd

@@ -109,6 +109,10 @@ struct mpd_solver {
     CUtensorMap tmap_pair[2];                // the same with 64-column tiles
     mpd::TmaPlan plan;                       // one-wave strips x bands
     mpd::TmaPlan pair_plan;                  // the same for lf_pair_kernel
+    int ring_overlap = 0;                    // fast steps: ring beside the interior (if ok)
+    bool overlap_ok = false;                 // bc_overlap_kernel fits beside the interior
+    int overlap_blocks = 0;                  // its grid: at most one block per SM
+    bool ring_beside = false;                // the interior just launched left the ring to it
     mpd::TmaPlan pplan;                      // persistent launch (cooperative wave)
     bool persist_ok = false;                 // the persistent engine can run here
     mpd::GridSync *gsync = nullptr;          // its barrier and reduction words
@@ -283,10 +287,14 @@ int InitFromIc(mpd_solver *s) {
 #define MPD_INTERIOR_PAIR 0
 #endif
 
+// alone: launches of the interior kernel with no boundary kernel after them
+// (per-kernel timing): the ring-beside form's rows and stores, with the
+// next launch let in only once a block's rows are done.
 int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool want_ws,
-                   int variant = MPD_INTERIOR_PAIR) {
+                   int variant = MPD_INTERIOR_PAIR, bool alone = false) {
     const mpd::Geo &g = s->g;
     const int usd = use_state_dt ? 1 : 0;
+    s->ring_beside = false;
     if (first || s->precision == MPD_PRECISION_EXACT) {
         dim3 block(32, 8);
         dim3 grid((g.M - 1 + 31) / 32, (g.L + 7) / 8);
@@ -301,8 +309,11 @@ int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool
                                    s->buf[1], s->st, dt, usd, want_ws, s->cphys, s->len,
                                    s->stream));
     } else {
+        const bool beside = s->ring_overlap && s->overlap_ok;
         MPD_CK(mpd::launch_lf_tma(g, s->plan, s->tmap[0], s->tmap[1], s->buf[0], s->buf[1],
-                                  s->st, dt, usd, want_ws, s->cphys, s->len, s->stream));
+                                  s->st, dt, usd, want_ws, beside, beside && !alone, s->cphys,
+                                  s->len, s->stream));
+        s->ring_beside = beside;
     }
     MPD_CK(cudaGetLastError());
     return MPD_OK;
@@ -311,6 +322,14 @@ int LaunchInterior(mpd_solver *s, bool first, bool use_state_dt, double dt, bool
 int LaunchBoundary(mpd_solver *s, bool use_state_dt, double dt) {
     const int nring = mpd::ring_count(s->g);
     const size_t smem = MPD_BC_SMEM_SEG ? s->bc.nseg_total * sizeof(mpd::SegDesc) : 0;
+    if (s->ring_beside) {
+        s->ring_beside = false;
+        MPD_CK(mpd::launch_pdl(mpd::bc_overlap_kernel, dim3(s->overlap_blocks), dim3(32),
+                               s->bc.nseg_total * sizeof(mpd::SegDesc), s->stream, s->g,
+                               s->buf[0], s->buf[1], (const double *)s->ic, s->bc, s->st, dt,
+                               use_state_dt ? 1 : 0, s->wall[0], s->wall[1], s->len));
+        return MPD_OK;
+    }
     MPD_CK(mpd::launch_pdl(mpd::bc_kernel, dim3((nring + kBcBlock - 1) / kBcBlock),
                            dim3(kBcBlock), smem, s->stream, s->g, s->buf[0], s->buf[1],
                            (const double *)s->ic, s->bc, s->st, dt, use_state_dt ? 1 : 0,
@@ -364,7 +383,7 @@ int CheckHandle(mpd_solver *s) {
 }
 
 int BuildGraph(mpd_solver *s, int steps, bool with_check, bool want_ws, int resid_every) {
-    const int key = (with_check ? 1 : 0) | (want_ws ? 2 : 0);
+    const int key = (with_check ? 1 : 0) | (want_ws ? 2 : 0) | (s->ring_overlap ? 4 : 0);
     if (s->graph && s->graph_steps == steps && s->graph_check == key &&
         s->graph_resid == resid_every)
         return MPD_OK;
@@ -543,6 +562,19 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
             mpd::plan_lf_pair(g, s->device, s->pair_plan) != cudaSuccess) {
             FreeAll(s);
             return Fail(MPD_ERR_CUDA, "occupancy query for the interior kernel failed");
+        }
+        {
+            // the ring beside the interior: rows 2..L-1 must exist; one block
+            // of one warp per SM at most, striding over the ring slots
+            int sms = 0;
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) !=
+                cudaSuccess) {
+                FreeAll(s);
+                return Fail(MPD_ERR_CUDA, "device query failed");
+            }
+            const int groups = (mpd::ring_count(g) + 31) / 32;
+            s->overlap_blocks = groups < sms ? groups : sms;
+            s->overlap_ok = g.L >= 4 && s->overlap_blocks > 0;
         }
         // the persistent engine needs cooperative launch and a strip per warp
         s->persist_ok = mpd::plan_lf_persist(g, s->device, s->pplan) == cudaSuccess;
@@ -1227,6 +1259,20 @@ int mpd_set_expression_ic(mpd_solver *s, const char *const exprs[8], int n_vars,
     return InitFromIc(s);
 }
 
+int mpd_set_ring_overlap(mpd_solver *s, int on) {
+    int rc = CheckHandle(s);
+    if (rc != MPD_OK) return rc;
+    MPD_CK(cudaStreamSynchronize(s->stream));
+    s->ring_overlap = on ? 1 : 0;
+    return MPD_OK;
+}
+
+int mpd_ring_overlap_active(mpd_solver *s, int *active) {
+    if (!s || !active) return Fail(MPD_ERR_INVALID, "bad arguments");
+    *active = (s->precision == MPD_PRECISION_FAST && s->ring_overlap && s->overlap_ok) ? 1 : 0;
+    return MPD_OK;
+}
+
 int mpd_get_stream(mpd_solver *s, void **stream) {
     if (!s || !stream) return Fail(MPD_ERR_INVALID, "bad arguments");
     *stream = static_cast<void *>(s->stream);
@@ -1284,9 +1330,9 @@ int mpd_profile_kernel(mpd_solver *s, int which, int launches, double dt, double
     MPD_CK(cudaEventRecord(s->ev0, s->stream));
     for (int i = 0; i < launches && rc == MPD_OK; ++i) {
         if (which == MPD_KERNEL_INTERIOR) {
-            rc = LaunchInterior(s, false, false, dt, true);
+            rc = LaunchInterior(s, false, false, dt, true, 0, true);
         } else if (which == MPD_KERNEL_INTERIOR_PAIR) {
-            rc = LaunchInterior(s, false, false, dt, true, 1);
+            rc = LaunchInterior(s, false, false, dt, true, 1, true);
         } else {
             mpd::residual_kernel<<<s->resid_blocks, 256, 0, s->stream>>>(s->g, s->buf[0],
                                                                          s->buf[1], s->st, 1);

@@ -288,6 +288,19 @@ class GpuSolver:
         self._call("mpd_get_stream", C.byref(s))
         return s.value or 0
 
+    @property
+    def ring_overlap(self) -> bool:
+        """Whether fast steps run the boundary ring beside the interior kernel
+        (bc_overlap_kernel) instead of after it (bc_kernel, the default); both
+        give the same bits.  Setting it takes effect from the next step."""
+        a = C.c_int()
+        self._call("mpd_ring_overlap_active", C.byref(a))
+        return bool(a.value)
+
+    @ring_overlap.setter
+    def ring_overlap(self, on: bool) -> None:
+        self._call("mpd_set_ring_overlap", 1 if on else 0)
+
     def profile_kernels(self, steps: int, dt: float):
         """Mean device ms per launch of (interior kernel, boundary kernel)."""
         out = np.zeros(2)
