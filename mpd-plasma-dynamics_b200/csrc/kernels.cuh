@@ -173,8 +173,9 @@ __device__ __forceinline__ void prefetch_l1(const void *p) {
 
 // Ahead of bc_ring_final's dependent chain for cell (l, m), touch the lines it
 // may read so that its loads hit this SM's L1: the central (unless they are
-// recomputed) and wall line entries next to the cell, the wall profiles of its rows and, on the axis
-// column, the u0 values of AxisLF.  A hint only: no value depends on it.
+// recomputed) and wall line entries next to the cell, the wall profiles of
+// its rows and, on the axis column, the u0 values of AxisLF.  A hint only: no
+// value depends on it.
 __device__ __forceinline__ void ring_prefetch(const BcView &v, int l, int m) {
     const Geo &g = v.g;
     const int L = g.L, M = g.M, len = v.len;
@@ -442,12 +443,15 @@ __global__ void MPD_BC_BOUNDS bc_kernel(Geo g, double *buf0, double *buf1,
 #endif
     pdl_wait();
     if (MPD_PDL_TRIG_BC == 1) pdl_trigger();
-    if (st->done) return;
+    // the step's state in one memory round trip
+    const int done = st->done;
     const long long step = st->step;
+    const double st_dt = st->dt;
+    const int flags = step_flags(st);
+    if (done) return;
     const double *u0 = (step & 1) ? buf1 : buf0;
     double *u = (step & 1) ? buf0 : buf1;
-    const double dt = use_state_dt ? st->dt : dt_arg;
-    const int flags = step_flags(st);
+    const double dt = use_state_dt ? st_dt : dt_arg;
     const BcView v = make_bc_view(g, u0, u, ic, cphys, (step & 1) ? wall1 : wall0, len,
                                   step == 0, fast, dt, bc);
     double *wnext = (step & 1) ? wall0 : wall1;
@@ -491,12 +495,14 @@ __global__ void __maxnreg__(MPD_OVERLAP_MAXNREG)
         __syncthreads();
         bc.seg = reinterpret_cast<const SegDesc *>(bc_smem_raw);
     }
-    if (__ldcg(&st->done)) return;
+    const int done = __ldcg(&st->done);
     const long long step = __ldcg(&st->step);
+    const double st_dt = __ldcg(&st->dt);
+    const int flags = __ldcg(&st->want_ws) ? kFlagWs : 0;
+    if (done) return;
     const double *u0 = (step & 1) ? buf1 : buf0;
     double *u = (step & 1) ? buf0 : buf1;
-    const double dt = use_state_dt ? __ldcg(&st->dt) : dt_arg;
-    const int flags = __ldcg(&st->want_ws) ? kFlagWs : 0;
+    const double dt = use_state_dt ? st_dt : dt_arg;
     BcView v = make_bc_view(g, u0, u, ic, nullptr, (step & 1) ? wall1 : wall0, len, step == 0,
                             1, dt, bc);
     v.recompute = 1;

@@ -331,12 +331,16 @@ __global__ void __launch_bounds__(32 * kTmaWarps, MPD_TMA_MINB)
     }
     pdl_wait();
     if (early_trigger) pdl_trigger();
-    if (st->done) return;
+    // the step's state in one memory round trip: all three loads issue
+    // before the branch
+    const int done = st->done;
     const long long step = st->step;
+    const double st_dt = st->dt;
+    if (done) return;
 
     TmaWarp w;
     tma_warp_setup(w, g, strip, (step & 1) ? buf0 : buf1, st, cphys, len,
-                   use_state_dt ? st->dt : dt_arg, (step & 1) ? &map1 : &map0);
+                   use_state_dt ? st_dt : dt_arg, (step & 1) ? &map1 : &map0);
     w.stage = reinterpret_cast<double *>(tma_smem) + wib * kTmaStages * kTmaRow;
     w.bar0 = bar0;
 
