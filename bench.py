@@ -78,7 +78,11 @@ def parse():
     ap.add_argument("--max-steps", type=int, default=200000)
     ap.add_argument("--surrogate", type=str, default="",
                     help="trained surrogate (.npz from --workload warmstart --save); "
-                         "without it serve trains a small one first")
+                         "without it serve trains a small one first; sweep takes a "
+                         "comma-separated list and predicts each draw with the one trained "
+                         "nearest its grid")
+    ap.add_argument("--skip-cold", action="store_true",
+                    help="sweep: leave out the cold batch (warm batch and plain march only)")
     ap.add_argument("--save", type=str, default="", help="warmstart: save the surrogate here")
     ap.add_argument("--big", type=str, default="4096x1600")
     ap.add_argument("--bootstrap", type=str, default="",
@@ -575,17 +579,18 @@ def run_serve(args):
 
 def run_sweep(args):
     """The north star's comparison on the parameter sweep of uneven grids:
-    batched cold, batched surrogate-warm (--surrogate, trained on a coarse
-    grid and interpolated onto each draw's grid) and the plain FP64 march one
-    solve after another (--plain-sample of the draws), all capped at
-    --max-steps.  value = warm batch solves/s."""
+    batched cold (unless --skip-cold), batched surrogate-warm (--surrogate:
+    each draw predicted by the surrogate trained nearest its grid,
+    interpolated onto the draw's grid) and the plain FP64 march one solve
+    after another (--plain-sample of the draws), all capped at --max-steps.
+    value = warm batch solves/s."""
     import __graft_entry__
     pkg = __graft_entry__.load_package()
     WS = pkg.warmstart
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
-    tr = WS.Trained.load(args.surrogate)
-    res = WS.sweep_comparison(tr, args.n_solves, args.max_steps, plain_sample=args.plain_sample,
-                              log=log)
+    trs = [WS.Trained.load(p) for p in args.surrogate.split(",") if p]
+    res = WS.sweep_comparison(trs, args.n_solves, args.max_steps, plain_sample=args.plain_sample,
+                              log=log, cold_batch=not args.skip_cold)
     return {"metric": "steady solves/s, warm-start batch on the uneven sweep",
             "value": res["warm_batch_solves_per_s"], "unit": "solves/s",
             "higher_is_better": True, "n_gpus": 1, "dtype": "f64 solver, bf16/f32 surrogate",

@@ -461,22 +461,57 @@ def run_pipeline(n_train=2000, n_eval=256, grid=(100, 40), epochs=40, batch=16, 
     return {**info, **res}
 
 
-def sweep_comparison(tr: Trained, n: int = 256, max_steps: int = 200_000, tol: float = 1e-8,
-                     plain_sample: int = 32, log=print) -> dict:
+def nearest_surrogate(trs: list, L: int) -> int:
+    """Index of the surrogate whose grid has the row count nearest to L (on a
+    log scale; a tie goes to the finer grid)."""
+    best, key = 0, None
+    for k, t in enumerate(trs):
+        d = (abs(np.log2(t.net.H / L)), -t.net.H)
+        if key is None or d < key:
+            best, key = k, d
+    return best
+
+
+def predicted_ics_nearest(trs: list, params: list[SweepParams]) -> tuple[list, float, list]:
+    """predicted_ics over several surrogates: each draw predicted by the one
+    trained nearest its grid (nearest_surrogate) and interpolated onto the
+    draw's grid.  Returns the planes, the inference seconds and the index of
+    the surrogate each draw used."""
+    pick = [nearest_surrogate(trs, p.L) for p in params]
+    ics: list = [None] * len(params)
+    infer_s = 0.0
+    for k, t in enumerate(trs):
+        idx = [i for i, q in enumerate(pick) if q == k]
+        if not idx:
+            continue
+        floor = t.floor if t.floor is not None else np.zeros(2)
+        got, s = predicted_ics(t, [params[i] for i in idx], None, floor)
+        infer_s += s
+        for i, g in zip(idx, got):
+            ics[i] = g
+    return ics, infer_s, pick
+
+
+def sweep_comparison(tr, n: int = 256, max_steps: int = 200_000, tol: float = 1e-8,
+                     plain_sample: int = 32, log=print, cold_batch: bool = True) -> dict:
     """The sweep of uneven grids (workloads.sweep_params(i), i < n) solved
     three ways, all capped at max_steps: the batched engine from the
-    workload's initial condition (cold), the batched engine from the
-    surrogate's prediction interpolated onto each draw's grid (warm, judged
-    and backed by the plain march: solve_warm with the full cap as budget),
-    and the plain FP64 march one solve after another on the first
-    plain_sample draws.  Rates count all solves and converged solves."""
+    workload's initial condition (cold; skipped with cold_batch=False), the
+    batched engine from a surrogate's prediction interpolated onto each
+    draw's grid (warm, judged and backed by the plain march: solve_warm with
+    the full cap as budget; tr is one Trained or a list, of which each draw
+    takes the one trained nearest its grid), and the plain FP64 march one
+    solve after another on the first plain_sample draws.  Rates count all
+    solves and converged solves."""
+    trs = list(tr) if isinstance(tr, (list, tuple)) else [tr]
     params = [sweep_params(i) for i in range(n)]
-    floor = tr.floor if tr.floor is not None else np.zeros(2)
-    ics, infer_s = predicted_ics(tr, params, None, floor)
-    cold = solve_all(params, max_steps=max_steps, tol=tol)
+    ics, infer_s, pick = predicted_ics_nearest(trs, params)
+    cold = solve_all(params, max_steps=max_steps, tol=tol) if cold_batch else None
     warm, fell = solve_warm(params, ics, max_steps=max_steps, tol=tol, budget=max_steps)
-    log(f"sweep of {n}: cold converged {int(cold.converged.sum())} in "
-        f"{cold.device_ms / 1e3:.1f} s, warm converged {int(warm.converged.sum())} in "
+    if cold is not None:
+        log(f"sweep of {n}: cold converged {int(cold.converged.sum())} in "
+            f"{cold.device_ms / 1e3:.1f} s")
+    log(f"sweep of {n}: warm converged {int(warm.converged.sum())} in "
         f"{warm.device_ms / 1e3:.1f} s ({int(fell.sum())} fell back)")
     seq_ms, seq_conv = 0.0, 0
     for p in params[:plain_sample]:
@@ -487,40 +522,55 @@ def sweep_comparison(tr: Trained, n: int = 256, max_steps: int = 200_000, tol: f
         seq_ms += r.device_ms
         seq_conv += int(r.converged)
         sv.close()
-    both = cold.converged & warm.converged
-    agree = [relative_linf(warm.fields[i], cold.fields[i]) for i in np.flatnonzero(both)]
+    agree = []
+    if cold is not None:
+        both = cold.converged & warm.converged
+        agree = [relative_linf(warm.fields[i], cold.fields[i]) for i in np.flatnonzero(both)]
     by_grid = {}
     for i, p in enumerate(params):
-        d = by_grid.setdefault(f"{p.L}x{p.M}", {"n": 0, "cold_converged": 0,
-                                                 "warm_converged": 0, "cold_steps": [],
-                                                 "warm_steps": []})
+        d = by_grid.setdefault(f"{p.L}x{p.M}", {
+            "n": 0, "cold_converged": 0, "warm_converged": 0, "cold_steps": [],
+            "warm_steps": [],
+            "surrogate_grid": f"{trs[pick[i]].net.H}x{trs[pick[i]].net.W - 1}"})
         d["n"] += 1
-        d["cold_converged"] += int(cold.converged[i])
         d["warm_converged"] += int(warm.converged[i])
-        d["cold_steps"].append(int(cold.steps[i]))
         d["warm_steps"].append(int(warm.steps[i]))
+        if cold is not None:
+            d["cold_converged"] += int(cold.converged[i])
+            d["cold_steps"].append(int(cold.steps[i]))
     for d in by_grid.values():
-        d["cold_steps_median"] = float(np.median(d.pop("cold_steps")))
+        cs = d.pop("cold_steps")
+        d["cold_steps_median"] = float(np.median(cs)) if cs else None
         d["warm_steps_median"] = float(np.median(d.pop("warm_steps")))
-    cold_s = cold.device_ms * 1e-3
+        if cold is None:
+            d["cold_converged"] = None
     warm_s = warm.device_ms * 1e-3 + infer_s
     seq_s = seq_ms * 1e-3
-    return {
+    out = {
         "n": n, "max_steps": max_steps, "tol": tol, "plain_sample": plain_sample,
-        "cold_batch_s": cold_s, "warm_batch_s": warm_s, "plain_sample_s": seq_s,
-        "cold_converged": int(cold.converged.sum()), "warm_converged": int(warm.converged.sum()),
+        "surrogate_grids": [f"{t.net.H}x{t.net.W - 1}" for t in trs],
+        "warm_batch_s": warm_s, "plain_sample_s": seq_s,
+        "warm_converged": int(warm.converged.sum()),
         "plain_sample_converged": seq_conv, "warm_fallbacks": int(fell.sum()),
-        "cold_batch_solves_per_s": n / cold_s, "warm_batch_solves_per_s": n / warm_s,
+        "warm_batch_solves_per_s": n / warm_s,
         "plain_solves_per_s": plain_sample / seq_s if seq_s > 0 else None,
-        "cold_batch_converged_per_s": int(cold.converged.sum()) / cold_s,
         "warm_batch_converged_per_s": int(warm.converged.sum()) / warm_s,
         "plain_converged_per_s": seq_conv / seq_s if seq_s > 0 else None,
         "warm_over_plain": (n / warm_s) / (plain_sample / seq_s) if seq_s > 0 else None,
+        "warm_over_plain_converged": ((int(warm.converged.sum()) / warm_s) /
+                                      (seq_conv / seq_s) if seq_s > 0 and seq_conv else None),
         "warm_vs_cold_state_rel_linf_max": np.stack(agree).max(0).tolist() if agree else None,
         "warm_p50_ms": float(np.percentile(warm.solve_ms, 50)),
         "warm_p99_ms": float(np.percentile(warm.solve_ms, 99)),
-        "cold_p50_ms": float(np.percentile(cold.solve_ms, 50)),
-        "cold_p99_ms": float(np.percentile(cold.solve_ms, 99)),
         "surrogate_inference_s": infer_s,
         "by_grid": by_grid,
     }
+    if cold is not None:
+        cold_s = cold.device_ms * 1e-3
+        out.update({
+            "cold_batch_s": cold_s, "cold_converged": int(cold.converged.sum()),
+            "cold_batch_solves_per_s": n / cold_s,
+            "cold_batch_converged_per_s": int(cold.converged.sum()) / cold_s,
+            "cold_p50_ms": float(np.percentile(cold.solve_ms, 50)),
+            "cold_p99_ms": float(np.percentile(cold.solve_ms, 99))})
+    return out

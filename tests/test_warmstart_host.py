@@ -38,3 +38,33 @@ def test_widened_draws_keep_the_sweep_box_stream():
         assert (p.amp, p.beta, p.vz) == (q.amp, q.beta, q.vz)
         assert q.a == p.a * 0.35 / 0.2 or abs(q.a - p.a * 1.75) < 1e-15
         assert 0.0 <= q.a < 0.35
+
+
+def test_interpolation_onto_a_coarser_grid_is_exact_for_linear_fields():
+    """A 400 x 160 prediction sampled onto a 200 x 80 draw (the sweep's finer
+    surrogate used for a coarser grid) keeps a field linear in (z, y)."""
+    Hc, Wc = 400, 161
+    z = np.arange(Hc) / Hc
+    y = np.arange(Wc) / (Wc - 1)
+    f = np.stack([(k + 1) * z[:, None] + 0.25 * k * y[None, :] for k in range(8)], -1)
+    g = WS.upsample_fields(f, 200, 80)
+    assert g.shape == (200, 81, 8)
+    zf, yf = np.arange(200) / 200, np.arange(81) / 80
+    for k in range(8):
+        np.testing.assert_allclose(g[..., k], (k + 1) * zf[:, None] + 0.25 * k * yf[None, :],
+                                   rtol=0, atol=1e-13)
+
+
+def test_each_draw_takes_the_surrogate_trained_nearest_its_grid():
+    class Net:
+        def __init__(self, H):
+            self.H, self.W = H, H // 4 + 1
+
+    class Tr:
+        def __init__(self, H):
+            self.net = Net(H)
+
+    trs = [Tr(100), Tr(400)]
+    assert [WS.nearest_surrogate(trs, L) for L in (100, 200, 400, 800)] == [0, 1, 1, 1]
+    assert WS.nearest_surrogate([Tr(100)], 800) == 0
+    assert [WS.nearest_surrogate([Tr(400), Tr(100)], L) for L in (100, 200)] == [1, 0]
