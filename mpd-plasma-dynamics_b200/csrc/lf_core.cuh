@@ -776,10 +776,13 @@ MPD_HD double bc_sym(const BcView &v, int idx, int l, int m, int ln, int mn, con
 }
 
 // An expression field the closed forms don't cover: full symbol table and
-// the bytecode interpreter.  Kept out of line so the common path stays small
-// and free of indexed local arrays.
-MPD_HD_NOINLINE double bc_eval_general(const BcView &v, int code, int l, int m, int ln, int mn,
-                                       Prim nb, Prim out) {
+// the bytecode interpreter.  Inlined: an out-of-line call takes the view by
+// reference, which puts the whole BcView in local memory for every caller
+// and turns each of its fields into a load on the boundary chains (the
+// boundary kernels' stacks shrink from 992 to 720 bytes, the batched
+// engine's spills from 594 to 314 bytes).
+MPD_HD double bc_eval_general(const BcView &v, int code, int l, int m, int ln, int mn,
+                              Prim nb, Prim out) {
     double sym[BS_COUNT];
     for (int t = 0; t < BS_COUNT; ++t) sym[t] = bc_sym(v, t, l, m, ln, mn, nb, out);
     return eval_code(v.bc.code + code, v.bc.consts, sym);
