@@ -137,6 +137,20 @@ def estimated_steps(cfg, max_steps: int) -> int:
     return int(min(max_steps, 4 * cfg.L_max ** 2))
 
 
+# Steps a surrogate-warm start of the channel takes to the same residual, per
+# grid row: the medians of the uneven sweep's warm solves on a B200 were
+# 2,951 / 8,651 / 11,551 / 26,551 steps at L = 100 / 200 / 400 / 800, about
+# 33 L (against the cold start's 4 L^2).  Only the batch plan uses it.
+WARM_STEPS_PER_ROW = 33
+
+
+def estimated_warm_steps(cfg, max_steps: int) -> int:
+    """Steps a surrogate-warm start needs (WARM_STEPS_PER_ROW L), capped at
+    max_steps: the batch plan's estimate for warm solves, which the cold law
+    (estimated_steps) overstates by 10-100x, the more so the finer the grid."""
+    return int(min(max_steps, WARM_STEPS_PER_ROW * cfg.L_max))
+
+
 class Autotuner:
     """Team sizes per grid shape from measured step times."""
 
@@ -167,12 +181,15 @@ class Autotuner:
         self.table[key] = out
         return out
 
-    def plan(self, cfgs, max_steps: int) -> BatchPlan:
+    def plan(self, cfgs, max_steps: int, estimate=estimated_steps) -> BatchPlan:
+        """Teams per grid shape.  estimate(cfg, max_steps): the steps a solve
+        is expected to take (cold law by default; estimated_warm_steps for
+        warm starts)."""
         shapes: dict[tuple[int, int], list[int]] = {}
         for i, c in enumerate(cfgs):
             shapes.setdefault((c.L_max, c.M_max), []).append(i)
         timing = {k: self.time_shape(cfgs[v[0]]) for k, v in shapes.items()}
-        steps = {k: max(estimated_steps(cfgs[i], max_steps) for i in v) for k, v in shapes.items()}
+        steps = {k: max(estimate(cfgs[i], max_steps) for i in v) for k, v in shapes.items()}
         # start: the block-efficient size (most cell-steps per block-second), one team
         state = {}
         for k, tab in timing.items():

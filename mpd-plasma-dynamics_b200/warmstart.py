@@ -32,7 +32,7 @@ import time
 import numpy as np
 
 from . import surrogate as S
-from .batch import Autotuner, BatchPlan, BatchSolver, estimated_steps
+from .batch import Autotuner, BatchPlan, BatchSolver, estimated_steps, estimated_warm_steps
 from .geometry import GeometryRegistry, Grid
 from .ic import ArrayIC, derived_pressures
 from .solver import GpuSolver, build_case
@@ -93,7 +93,8 @@ class SolveSet:
 
 
 def solve_all(params: list[SweepParams], ics: list | None = None, max_steps=200_000, tol=1e-8,
-              every=50, chunk: int = 256, tuner: Autotuner | None = None) -> SolveSet:
+              every=50, chunk: int = 256, tuner: Autotuner | None = None,
+              estimate=None) -> SolveSet:
     """Solve every draw with the batched engine, in batches of at most `chunk`
     solves, from the workload's initial condition (the workload's dt0) or,
     with ics, from the given planes starting at their CFL dt: the LF steady
@@ -118,7 +119,9 @@ def solve_all(params: list[SweepParams], ics: list | None = None, max_steps=200_
                 solvers.append(GpuSolver(cfg, grid_of(cfg), ic, precision="fast"))
         batch = BatchSolver(solvers)
         tuner = tuner or Autotuner(batch.capacity, steps=100)
-        plan = tuner.plan(cfgs, max_steps=max_steps)
+        if estimate is None:
+            estimate = estimated_steps if ics is None else estimated_warm_steps
+        plan = tuner.plan(cfgs, max_steps=max_steps, estimate=estimate)
         out = batch.run(plan, dt=None if ics is None else 0.0, max_steps=max_steps,
                         residual_tol=tol, residual_every=every)
         dev_ms += out.device_ms

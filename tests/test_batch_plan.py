@@ -77,3 +77,19 @@ def test_plan_rejects_shapes_beyond_one_wave(pkg):
     cfgs = _batch(1)
     with pytest.raises(ValueError):
         _tuner(pkg, 3, TABLE).plan(cfgs, max_steps=20000)
+
+
+def test_warm_estimate_plans_for_the_warm_makespan(pkg):
+    """Warm solves take about 33 L steps, not the cold 4 L^2: planned with
+    the warm estimate, the batch's makespan under warm step counts is no
+    worse than the cold law's plan, and strictly better at a large cap."""
+    cfgs = _batch(16)
+    cap = 2_500_000
+    warm = lambda c: pkg.batch.estimated_warm_steps(c, cap)
+    assert [warm(_cfg(*k)) for k in TABLE] == [3300, 6600, 13200, 26400]
+    tuner = _tuner(pkg, 444, TABLE)
+    plan_cold = tuner.plan(cfgs, max_steps=cap)
+    plan_warm = tuner.plan(cfgs, max_steps=cap, estimate=pkg.batch.estimated_warm_steps)
+    span_cold = _makespan(plan_cold, cfgs, TABLE, warm)
+    span_warm = _makespan(plan_warm, cfgs, TABLE, warm)
+    assert span_warm < span_cold
