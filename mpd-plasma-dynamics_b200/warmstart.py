@@ -31,6 +31,7 @@ import time
 
 import numpy as np
 
+from . import _native as N
 from . import surrogate as S
 from .batch import Autotuner, BatchPlan, BatchSolver, estimated_steps, estimated_warm_steps
 from .geometry import GeometryRegistry, Grid
@@ -517,6 +518,7 @@ def sweep_comparison(tr, n: int = 256, max_steps: int = 200_000, tol: float = 1e
     log(f"sweep of {n}: warm converged {int(warm.converged.sum())} in "
         f"{warm.device_ms / 1e3:.1f} s ({int(fell.sum())} fell back)")
     seq_ms, seq_conv = 0.0, 0
+    plain_end = {"converged": 0, "nonfinite": 0, "capped": 0, "other": 0}
     for p in params[:plain_sample]:
         cfg = p.config()
         sv = build_case(cfg, precision="fast")
@@ -524,6 +526,9 @@ def sweep_comparison(tr, n: int = 256, max_steps: int = 200_000, tol: float = 1e
                    residual_every=50, engine="graph")
         seq_ms += r.device_ms
         seq_conv += int(r.converged)
+        plain_end["converged" if r.converged else
+                  "nonfinite" if r.status == N.MPD_ERR_NONFINITE else
+                  "capped" if r.steps >= max_steps else "other"] += 1
         sv.close()
     agree = []
     if cold is not None:
@@ -554,7 +559,8 @@ def sweep_comparison(tr, n: int = 256, max_steps: int = 200_000, tol: float = 1e
         "surrogate_grids": [f"{t.net.H}x{t.net.W - 1}" for t in trs],
         "warm_batch_s": warm_s, "plain_sample_s": seq_s,
         "warm_converged": int(warm.converged.sum()),
-        "plain_sample_converged": seq_conv, "warm_fallbacks": int(fell.sum()),
+        "plain_sample_converged": seq_conv, "plain_sample_ends": plain_end,
+        "warm_fallbacks": int(fell.sum()),
         "warm_batch_solves_per_s": n / warm_s,
         "plain_solves_per_s": plain_sample / seq_s if seq_s > 0 else None,
         "warm_batch_converged_per_s": int(warm.converged.sum()) / warm_s,
