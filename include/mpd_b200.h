@@ -177,7 +177,9 @@ typedef struct mpd_run_stats {
     double max_wave_speed;
     int converged;       /* 1 = residual or change criterion met */
     int status;          /* MPD_OK or MPD_ERR_NONFINITE          */
-    double device_ms;    /* device time of the loop (CUDA events) */
+    double device_ms;    /* device time of the loop (CUDA events on the handle's stream,
+                            from before the first launch to the end of the launch the
+                            run stopped in) */
 } mpd_run_stats;
 
 int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats);

@@ -121,6 +121,8 @@ struct mpd_solver {
     mpd::DevState *h_st = nullptr;  // pinned mirror
     mpd::DevState *h_ring = nullptr;  // pinned: the state after each in-flight graph launch
     cudaEvent_t ev_ring[2] = {nullptr, nullptr};
+    cudaEvent_t ev_end[2] = {nullptr, nullptr};  // timing: end of each in-flight launch's work
+    cudaEvent_t ev_stop = nullptr;               // ev_end of the launch the run stopped in
     mpd::HostMirror *hm = nullptr;   // mapped pinned: the controller's per-step outputs
     cudaEvent_t ev_sync = nullptr;   // completion of the enqueued work, for hm
     mpd::SegDesc *d_seg = nullptr;
@@ -187,6 +189,8 @@ void FreeAll(mpd_solver *s) {
     cudaFree(s->d_consts);
     if (s->h_st) cudaFreeHost(s->h_st);
     if (s->h_ring) cudaFreeHost(s->h_ring);
+    for (cudaEvent_t e : s->ev_end)
+        if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : s->ev_ring)
         if (e) cudaEventDestroy(e);
     if (s->hm) cudaFreeHost(s->hm);
@@ -500,6 +504,7 @@ int mpd_create(const mpd_config *cfg, const mpd_geometry *geom, const double *ph
             cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_ring[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_ring[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&s->ev_end[0]) != cudaSuccess || cudaEventCreate(&s->ev_end[1]) != cudaSuccess ||
         cudaHostAlloc(reinterpret_cast<void **>(&s->hm), sizeof(mpd::HostMirror),
                       cudaHostAllocMapped) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_sync, cudaEventDisableTiming) != cudaSuccess) {
@@ -630,10 +635,18 @@ int mpd_advance(mpd_solver *s, double dt) {
 static int FinishRun(mpd_solver *s, long long step0, mpd_run_stats *stats) {
     mpd::DevState &h = *s->h_st;
     int rc = MPD_OK;
-    MPD_CK(cudaEventRecord(s->ev1, s->stream));
-    MPD_CK(cudaEventSynchronize(s->ev1));
+    // device time: to the end of the graph launch the run stopped in (the
+    // host learns of the stop only later, through the launch's state copy),
+    // else to an event recorded now (the persistent engine)
+    cudaEvent_t end = s->ev_stop;
+    s->ev_stop = nullptr;
+    if (!end) {
+        MPD_CK(cudaEventRecord(s->ev1, s->stream));
+        end = s->ev1;
+    }
+    MPD_CK(cudaEventSynchronize(end));
     float ms = 0.f;
-    MPD_CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    MPD_CK(cudaEventElapsedTime(&ms, s->ev0, end));
     rc = SyncState(s);  // the loop read the controller through its own slots
     if (rc != MPD_OK) return rc;
     // the residual of the final state, when the loop stopped between checks
@@ -769,6 +782,7 @@ static int GraphLoop(mpd_solver *s, long long budget, int per_graph) {
     int pending = 0;
     auto launch = [&](int slot) -> int {
         MPD_CK(cudaGraphLaunch(s->graph, s->stream));
+        MPD_CK(cudaEventRecord(s->ev_end[slot], s->stream));
         MPD_CK(cudaMemcpyAsync(&s->h_ring[slot], s->st, sizeof(mpd::DevState),
                                cudaMemcpyDeviceToHost, s->stream));
         MPD_CK(cudaEventRecord(s->ev_ring[slot], s->stream));
@@ -790,7 +804,10 @@ static int GraphLoop(mpd_solver *s, long long budget, int per_graph) {
             MPD_CK(cudaStreamSynchronize(s->stream));
             return Fail(MPD_ERR_TIMEOUT, "a bounded device wait gave up; the state is not valid");
         }
-        if (r.done) return MPD_OK;  // a launch still in flight exits at once
+        if (r.done) {  // a launch still in flight exits at once
+            s->ev_stop = s->ev_end[slot];
+            return MPD_OK;
+        }
         if (r.step == last_step) {  // a launch that advanced nothing: stop, don't spin
             MPD_CK(cudaStreamSynchronize(s->stream));
             return Fail(MPD_ERR_TIMEOUT, "run loop made no progress");
@@ -860,6 +877,7 @@ int mpd_run(mpd_solver *s, const mpd_run_params *p, mpd_run_stats *stats) {
     if (rc != MPD_OK) return rc;
     mpd::DevState &h = *s->h_st;
 
+    s->ev_stop = nullptr;
     MPD_CK(cudaEventRecord(s->ev0, s->stream));
     if (!h.done && s->host_step == 0) {
         rc = EnqueueStep(s, true, true, 0.0, with_check, want_ws, p->residual_every == 1);
