@@ -1561,9 +1561,9 @@ int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *
         // Elastic re-plan: once fewer solves are left than teams (the rest
         // would idle for the remaining launches), every remaining solve gets
         // a team of its own and the wave's blocks are split evenly between
-        // them, up to the blocks that still give it interior tasks (64 at
-        // most: beyond that the team barriers cost more than the tasks
-        // give).  A solve's results do not depend on its team's size.
+        // them, up to the blocks that still give it interior tasks (one
+        // 800 x 320 solve on a B200: 50.6 us a step on 64 blocks, 33.8 us on
+        // 128).  A solve's results do not depend on its team's size.
         std::vector<int> active;
         for (int i = 0; i < n; ++i)
             if (!b->solvers[i]->h_st->done) active.push_back(i);
@@ -1575,8 +1575,7 @@ int mpd_batch_run(mpd_batch *b, const mpd_run_params *p, int nteams, const int *
                 mpd_solver *sv = b->solvers[active[k]];
                 const int strips = (sv->M + mpd::kFastCells - 1) / mpd::kFastCells;
                 const long long tasks = static_cast<long long>(strips) * sv->L;
-                int want = static_cast<int>((tasks + mpd::kTmaWarps - 1) / mpd::kTmaWarps);
-                want = want < 64 ? want : 64;
+                const int want = static_cast<int>((tasks + mpd::kTmaWarps - 1) / mpd::kTmaWarps);
                 int nb = share < want ? share : want;
                 if (nb < 1) nb = 1;
                 tf[k + 1] = tf[k] + nb;
