@@ -102,3 +102,28 @@ def test_untrained_surrogate_falls_back_to_cold_start():
         np.testing.assert_array_equal(warm.fields[i], cold.fields[i])
     for i in np.flatnonzero(~fell):
         assert warm.converged[i] and warm.steps[i] <= budget
+
+
+def test_each_draw_is_predicted_by_the_nearest_surrogate():
+    """Two surrogates on different grids (untrained: only the routing is
+    checked): each draw's prediction comes from the one trained nearest its
+    grid and is interpolated onto the draw's own grid, so it equals that
+    surrogate's prediction alone, in the draw's shape."""
+    WS, S = pkg.warmstart, pkg.surrogate
+    rng = np.random.default_rng(0)
+    Y = rng.standard_normal((4, 1, S.N_OUT)) * 0.1 + 1.0
+    trs = []
+    for H, W in ((24, 11), (96, 41)):
+        net = S.SpectralOperator(H, W, 16, seed=H)
+        trs.append(WS.Trained(net, S.Normalizer.fit(Y), [], 0.0, np.array([1e-3, 1e-3])))
+    params = [WS.SweepParams(L, M, 1.0, 0.2, 0.1, 0.05)
+              for L, M in ((24, 10), (48, 20), (96, 40), (192, 80))]
+    ics, _, pick = WS.predicted_ics_nearest(trs, params)
+    assert pick == [0, 1, 1, 1]
+    for p, ic, k in zip(params, ics, pick):
+        alone, _ = WS.predicted_ics(trs[k], [p], None, trs[k].floor)
+        if alone[0] is None:
+            assert ic is None
+            continue
+        assert ic.shape == alone[0].shape
+        np.testing.assert_array_equal(ic, alone[0])
