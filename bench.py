@@ -346,9 +346,14 @@ def run_ours(args, rank, world, local_rank):
     # per-launch device time of the dominant kernel and of the residual pass:
     # back-to-back launches between two events on the solver's stream
     hbm, hbm_src = measured_hbm()
-    int_ms = solver.profile_kernel("interior", 30, res.dt)
-    int2_ms = solver.profile_kernel("interior_pair", 30, res.dt)
-    resid_ms = solver.profile_kernel("residual", 30, res.dt)
+    # median of five samples of 30 launches each: one sample varies by up
+    # to 8 % between runs on the same GPU
+    def kernel_ms(which):
+        return statistics.median(solver.profile_kernel(which, 30, res.dt) for _ in range(5))
+
+    int_ms = kernel_ms("interior")
+    int2_ms = kernel_ms("interior_pair")
+    resid_ms = kernel_ms("residual")
     ring_beside = solver.ring_overlap
     int_bytes = ALG_BYTES_PER_CELL * interior_cells(ring_beside)
     achieved = int_bytes / (int_ms * 1e-3) / 1e9
@@ -438,14 +443,14 @@ def run_ours(args, rank, world, local_rank):
                          "pair_kernel_ms": int2_ms,
                          "alg_bytes_per_launch": int_bytes,
                          "ring_beside_interior": ring_beside,
-                         "kernel_timing": "30 back-to-back launches between two CUDA events",
+                         "kernel_timing": "median of 5 samples of 30 back-to-back launches between two CUDA events",
                          "peak_source": hbm_src},
             "residual_kernel": {"kernel": "residual_kernel", "ms": resid_ms,
                                 "achieved": resid_gbs, "unit": "GB/s", "peak": hbm,
                                 "frac": resid_gbs / hbm,
                                 "traffic": profiled_traffic("residual_kernel")[0],
                                 "alg_bytes_per_launch": RESID_BYTES_PER_CELL * CELLS,
-                                "how": "30 back-to-back launches between two CUDA events"},
+                                "how": "median of 5 samples of 30 back-to-back launches between two CUDA events"},
             "cpu_baseline": cpu,
             "e2e": {"value": world * CELLS * n_e2e / e2e_s, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
