@@ -583,7 +583,7 @@ def run_serve(args):
 
 
 def run_sweep(args):
-    """The north star's comparison on the parameter sweep of uneven grids:
+    """The warm-start comparison on the parameter sweep of uneven grids:
     batched cold (unless --skip-cold), batched surrogate-warm (--surrogate:
     each draw predicted by the surrogate trained nearest its grid,
     interpolated onto the draw's grid) and the plain FP64 march one solve
