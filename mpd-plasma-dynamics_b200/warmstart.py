@@ -496,6 +496,23 @@ def predicted_ics_nearest(trs: list, params: list[SweepParams]) -> tuple[list, f
     return ics, infer_s, pick
 
 
+def stratified_sample(params: list[SweepParams], k: int) -> list[int]:
+    """Indices of k draws with the grid mix of the whole list: per grid, its
+    share of k (largest remainders rounded up), taken as that grid's first
+    draws in list order."""
+    groups: dict[tuple[int, int], list[int]] = {}
+    for i, p in enumerate(params):
+        groups.setdefault((p.L, p.M), []).append(i)
+    n = len(params)
+    k = min(k, n)
+    want = {g: k * len(v) / n for g, v in groups.items()}
+    take = {g: int(math.floor(w)) for g, w in want.items()}
+    left = k - sum(take.values())
+    for g in sorted(want, key=lambda g: (take[g] - want[g], g))[:left]:
+        take[g] += 1
+    return sorted(i for g, v in groups.items() for i in v[:take[g]])
+
+
 def sweep_comparison(tr, n: int = 256, max_steps: int = 200_000, tol: float = 1e-8,
                      plain_sample: int = 32, log=print, cold_batch: bool = True) -> dict:
     """The sweep of uneven grids (workloads.sweep_params(i), i < n) solved
@@ -505,8 +522,8 @@ def sweep_comparison(tr, n: int = 256, max_steps: int = 200_000, tol: float = 1e
     draw's grid (warm, judged and backed by the plain march: solve_warm with
     the full cap as budget; tr is one Trained or a list, of which each draw
     takes the one trained nearest its grid), and the plain FP64 march one
-    solve after another on the first plain_sample draws.  Rates count all
-    solves and converged solves."""
+    solve after another on plain_sample draws with the sweep's grid mix
+    (stratified_sample).  Rates count all solves and converged solves."""
     trs = list(tr) if isinstance(tr, (list, tuple)) else [tr]
     params = [sweep_params(i) for i in range(n)]
     ics, infer_s, pick = predicted_ics_nearest(trs, params)
@@ -519,16 +536,25 @@ def sweep_comparison(tr, n: int = 256, max_steps: int = 200_000, tol: float = 1e
         f"{warm.device_ms / 1e3:.1f} s ({int(fell.sum())} fell back)")
     seq_ms, seq_conv = 0.0, 0
     plain_end = {"converged": 0, "nonfinite": 0, "capped": 0, "other": 0}
-    for p in params[:plain_sample]:
+    plain_by_grid: dict[str, dict] = {}
+    for i in stratified_sample(params, plain_sample):
+        p = params[i]
         cfg = p.config()
         sv = build_case(cfg, precision="fast")
         r = sv.run(T=1e300, dt=cfg.dt, adaptive=True, max_steps=max_steps, residual_tol=tol,
                    residual_every=50, engine="graph")
         seq_ms += r.device_ms
         seq_conv += int(r.converged)
-        plain_end["converged" if r.converged else
-                  "nonfinite" if r.status == N.MPD_ERR_NONFINITE else
-                  "capped" if r.steps >= max_steps else "other"] += 1
+        end = ("converged" if r.converged else
+               "nonfinite" if r.status == N.MPD_ERR_NONFINITE else
+               "capped" if r.steps >= max_steps else "other")
+        plain_end[end] += 1
+        d = plain_by_grid.setdefault(f"{p.L}x{p.M}", {"n": 0, "converged": 0, "nonfinite": 0,
+                                                      "seconds": 0.0})
+        d["n"] += 1
+        d["converged"] += int(r.converged)
+        d["nonfinite"] += int(end == "nonfinite")
+        d["seconds"] += r.device_ms * 1e-3
         sv.close()
     agree = []
     if cold is not None:
@@ -560,6 +586,7 @@ def sweep_comparison(tr, n: int = 256, max_steps: int = 200_000, tol: float = 1e
         "warm_batch_s": warm_s, "plain_sample_s": seq_s,
         "warm_converged": int(warm.converged.sum()),
         "plain_sample_converged": seq_conv, "plain_sample_ends": plain_end,
+        "plain_sample_by_grid": plain_by_grid,
         "warm_fallbacks": int(fell.sum()),
         "warm_batch_solves_per_s": n / warm_s,
         "plain_solves_per_s": plain_sample / seq_s if seq_s > 0 else None,

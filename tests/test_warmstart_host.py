@@ -68,3 +68,19 @@ def test_each_draw_takes_the_surrogate_trained_nearest_its_grid():
     assert [WS.nearest_surrogate(trs, L) for L in (100, 200, 400, 800)] == [0, 1, 1, 1]
     assert WS.nearest_surrogate([Tr(100)], 800) == 0
     assert [WS.nearest_surrogate([Tr(400), Tr(100)], L) for L in (100, 200)] == [1, 0]
+
+
+def test_plain_sample_has_the_sweeps_grid_mix():
+    params = [WS.sweep_params(i) for i in range(256)]
+    idx = WS.stratified_sample(params, 32)
+    assert len(idx) == 32 and len(set(idx)) == 32 and idx == sorted(idx)
+    from collections import Counter
+    full = Counter((p.L, p.M) for p in params)
+    got = Counter((params[i].L, params[i].M) for i in idx)
+    for g, c in full.items():
+        assert abs(got[g] - 32 * c / 256) < 1.0
+    # each grid's first draws
+    for g in full:
+        mine = [i for i in idx if (params[i].L, params[i].M) == g]
+        first = [i for i, p in enumerate(params) if (p.L, p.M) == g][:len(mine)]
+        assert mine == first
